@@ -1,0 +1,108 @@
+/*
+ * shafft_sm100.h -- C ABI of the B200 (sm_100a) C2C FFT kernel library,
+ * libshafft_sm100.so.
+ *
+ * This is the thin layer the SHAFFT host library (libshafft.so, which keeps
+ * the reference's FFTND/FFT1D classes and C API) reaches the CUDA kernels
+ * through.  Plain pointers, sizes and int status codes; no exceptions, no
+ * C++ or torch types.
+ *
+ * Each entry point replaces a backend "method" call of the reference
+ * (paths relative to the SHAFFT project):
+ *   shafft_sm100_plan_create_nd  <- fftndPlan      src/cpp/fft/hipfft_method/fftnd_method.cpp:162-351
+ *                                   (hipfftMakePlanMany64 at :323-335)
+ *   shafft_sm100_plan_create_1d  <- fft1dPlan      src/cpp/fft/hipfft_method/fft1d_method.hip:416-581
+ *   shafft_sm100_execute         <- fftndExecute   src/cpp/fft/hipfft_method/fftnd_method.cpp:371-533
+ *                                   (hipfftExecC2C/Z2Z at :486-497) and
+ *                                   fft1dExecute   src/cpp/fft/hipfft_method/fft1d_method.hip:628-650
+ *   shafft_sm100_scale           <- normalizeComplexFloat/Double
+ *                                   src/cpp/fft/hipfft_method/common/normalize.hip:41-77
+ *   shafft_sm100_plan_destroy    <- fftndDestroy / fft1dDestroy
+ *   shafft_sm100_set_stream      <- fftndSetStream src/cpp/fft/hipfft_method/fftnd_method.cpp:353-369
+ *
+ * Conventions: row-major, last axis fastest; forward = exp(-2*pi*i*jk/n);
+ * execute is unnormalised unless a scale != 1 is passed (the fused
+ * normalisation of the last pass).  Element types: precision 0 = complex64
+ * (interleaved float re/im), 1 = complex128 (interleaved double).
+ *
+ * Return codes: 0 success, otherwise one of SHAFFT_SM100_E*.
+ */
+#ifndef SHAFFT_SM100_H
+#define SHAFFT_SM100_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHAFFT_SM100_OK 0
+#define SHAFFT_SM100_EINVAL 1   /* bad argument (null pointer, size, dims)   */
+#define SHAFFT_SM100_EALLOC 2   /* device allocation failed                  */
+#define SHAFFT_SM100_ECUDA 3    /* CUDA runtime error (see last_cuda_error)  */
+#define SHAFFT_SM100_ENOTSUP 4  /* size outside what the planner can handle  */
+
+typedef struct shafft_sm100_plan_s* shafft_sm100_plan;
+
+/* Plan a C2C transform over every axis of a row-major tensor dims[0..ndim).
+ * Builds twiddle / chirp / permutation tables on the current device (FP64
+ * generation) and allocates plan-owned scratch when Bluestein stages need it.
+ * Synchronous with respect to the host. */
+int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t* dims,
+                                int precision);
+
+/* Plan a 1-D C2C transform of length n (equivalent to the 1-D ND plan). */
+int shafft_sm100_plan_create_1d(shafft_sm100_plan* out, int64_t n, int precision);
+
+int shafft_sm100_plan_destroy(shafft_sm100_plan plan);
+
+/* Default stream for shafft_sm100_execute calls that pass stream == NULL. */
+int shafft_sm100_set_stream(shafft_sm100_plan plan, void* stream /* cudaStream_t */);
+
+/* Execute: src -> dst.  direction 0 = forward, 1 = backward.  The output is
+ * multiplied by `scale` (pass 1.0 for the unnormalised transform).  src and
+ * dst must be distinct device buffers of at least plan_elements() complex
+ * elements; src's contents are undefined afterwards (it is used as
+ * ping-pong space).  Asynchronous: enqueued on `stream` (cudaStream_t; NULL
+ * selects the plan's stream). */
+int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direction, double scale,
+                         void* stream);
+
+/* data[i] *= factor over count complex elements (stand-alone normalize). */
+int shafft_sm100_scale(void* data, size_t count, int precision, double factor, void* stream);
+
+/* Number of complex elements of the transform. */
+int64_t shafft_sm100_plan_elements(shafft_sm100_plan plan);
+
+/* Number of full HBM passes one execute performs (kernel launches that
+ * read and write the whole tensor, counting elementwise Bluestein steps). */
+int shafft_sm100_plan_passes(shafft_sm100_plan plan);
+
+/* Number of kernel launches one execute performs. */
+int shafft_sm100_plan_launches(shafft_sm100_plan plan);
+
+/* Plan-owned device bytes (tables + scratch). */
+size_t shafft_sm100_plan_device_bytes(shafft_sm100_plan plan);
+
+/* Host-only planning query (no device needed): writes a JSON description of
+ * the pass list for the given shape into buf.  Returns the status code. */
+int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* buf, int buflen);
+
+/* JSON description of a created plan. */
+int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen);
+
+/* Last CUDA runtime error code seen by this library on this thread. */
+int shafft_sm100_last_cuda_error(void);
+
+/* Human-readable message for the last error on this thread. */
+const char* shafft_sm100_last_error_message(void);
+
+/* Library version string. */
+const char* shafft_sm100_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHAFFT_SM100_H */

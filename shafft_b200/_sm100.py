@@ -1,0 +1,119 @@
+"""ctypes binding of libshafft_sm100.so (the kernel library's C ABI,
+include/shafft_sm100.h).
+
+The product path is C/C++/CUDA; this module only forwards plain pointers
+and sizes.  It fails loudly when the shared library has not been built:
+there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+LIB_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+SM100_LIB = os.path.join(LIB_DIR, "libshafft_sm100.so")
+
+_lib = None
+
+
+class Sm100Error(RuntimeError):
+    pass
+
+
+def load():
+    """Load libshafft_sm100.so (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(SM100_LIB):
+        raise Sm100Error(
+            f"{SM100_LIB} is not built; run __graft_entry__.build() "
+            "(python -c 'import __graft_entry__ as g; g.build()')")
+    lib = ctypes.CDLL(SM100_LIB, mode=ctypes.RTLD_GLOBAL)
+    vp = ctypes.c_void_p
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    lib.shafft_sm100_plan_create_nd.argtypes = [ctypes.POINTER(vp), ctypes.c_int, i64p, ctypes.c_int]
+    lib.shafft_sm100_plan_create_1d.argtypes = [ctypes.POINTER(vp), ctypes.c_int64, ctypes.c_int]
+    lib.shafft_sm100_plan_destroy.argtypes = [vp]
+    lib.shafft_sm100_set_stream.argtypes = [vp, vp]
+    lib.shafft_sm100_execute.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, vp]
+    lib.shafft_sm100_scale.argtypes = [vp, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, vp]
+    lib.shafft_sm100_plan_elements.argtypes = [vp]
+    lib.shafft_sm100_plan_elements.restype = ctypes.c_int64
+    lib.shafft_sm100_plan_passes.argtypes = [vp]
+    lib.shafft_sm100_plan_launches.argtypes = [vp]
+    lib.shafft_sm100_plan_device_bytes.argtypes = [vp]
+    lib.shafft_sm100_plan_device_bytes.restype = ctypes.c_size_t
+    lib.shafft_sm100_plan_query.argtypes = [ctypes.c_int, i64p, ctypes.c_int, ctypes.c_char_p,
+                                            ctypes.c_int]
+    lib.shafft_sm100_plan_describe.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    lib.shafft_sm100_last_error_message.restype = ctypes.c_char_p
+    lib.shafft_sm100_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = load().shafft_sm100_last_error_message().decode(errors="replace")
+        raise Sm100Error(f"{what} failed rc={rc}: {msg}")
+
+
+def plan_query(dims, precision=0) -> dict:
+    """Host-only planner query (no GPU needed)."""
+    lib = load()
+    d = (ctypes.c_int64 * len(dims))(*dims)
+    buf = ctypes.create_string_buffer(1 << 16)
+    _check(lib.shafft_sm100_plan_query(len(dims), d, precision, buf, len(buf)), "plan_query")
+    return json.loads(buf.value.decode())
+
+
+class Plan:
+    """Owning handle of a shafft_sm100 plan (device tables + scratch)."""
+
+    def __init__(self, dims, precision=0):
+        lib = load()
+        self._lib = lib
+        self.dims = tuple(int(x) for x in dims)
+        self.precision = int(precision)
+        h = ctypes.c_void_p()
+        d = (ctypes.c_int64 * len(self.dims))(*self.dims)
+        _check(lib.shafft_sm100_plan_create_nd(ctypes.byref(h), len(self.dims), d, self.precision),
+               "plan_create_nd")
+        self.handle = h
+
+    def execute(self, src_ptr: int, dst_ptr: int, direction: int = 0, scale: float = 1.0,
+                stream: int = 0):
+        _check(self._lib.shafft_sm100_execute(self.handle, ctypes.c_void_p(src_ptr),
+                                              ctypes.c_void_p(dst_ptr), int(direction),
+                                              float(scale), ctypes.c_void_p(stream)), "execute")
+
+    def describe(self) -> dict:
+        buf = ctypes.create_string_buffer(1 << 16)
+        _check(self._lib.shafft_sm100_plan_describe(self.handle, buf, len(buf)), "describe")
+        return json.loads(buf.value.decode())
+
+    @property
+    def launches(self) -> int:
+        return self._lib.shafft_sm100_plan_launches(self.handle)
+
+    @property
+    def passes(self) -> int:
+        return self._lib.shafft_sm100_plan_passes(self.handle)
+
+    def destroy(self):
+        if self.handle:
+            self._lib.shafft_sm100_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def scale(ptr: int, count: int, precision: int, factor: float, stream: int = 0):
+    _check(load().shafft_sm100_scale(ctypes.c_void_p(ptr), count, precision, factor,
+                                     ctypes.c_void_p(stream)), "scale")

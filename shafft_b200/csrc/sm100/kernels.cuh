@@ -1,0 +1,321 @@
+// Device kernels of the sm_100a C2C FFT backend.
+//
+// k_fft_pass  -- one HBM pass: batched length-L DFTs on W-wide tiles.
+//   Phase 1: each thread loads the R inputs of a first-stage butterfly
+//            straight from HBM (coalesced: lanes walk b0 for column tiles or
+//            n for row tiles), applies input conjugation / four-step
+//            pre-twiddle, runs the radix-R butterfly in registers, applies
+//            the decimation-in-frequency twiddle and writes the R results to
+//            shared memory in place.
+//   Phase 2: the remaining radix stages run in shared memory, in place
+//            (Cooley-Tukey DIF; span shrinks by the stage radix).  The
+//            shared tile is [L][W] with an odd row pitch (W+1), so 16 lanes
+//            that share a row and differ in w never hit the same bank, and
+//            16 lanes that walk rows with a fixed w do not either.
+//   Phase 3: results are read back in digit-reversed order through a small
+//            permutation table and stored to HBM with the four-step
+//            post-twiddle, scale and output conjugation fused in.
+// The same source serves a runtime length (LS == 0) and compile-time
+// specialisations for the hot lengths, where all index arithmetic folds.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "butterflies.cuh"
+#include "pass.h"
+
+namespace shafft_sm100 {
+
+template <typename C>
+__device__ __forceinline__ C tw_n(const PassTables<C>& tb, int shift, int64_t mask, int64_t m) {
+  C hi = tb.tw_hi[m >> shift];
+  C lo = tb.tw_lo[m & mask];
+  return cmul(hi, lo);
+}
+
+template <int R, typename C>
+__device__ __forceinline__ void stage_first(const PassGeom& g, const PassTables<C>& tb, const C* in,
+                                            C* sm, int L, int W, int logW, int pitch, int nst,
+                                            int wcount, int64_t bin, int64_t w0, int64_t tconst) {
+  const int m0 = L / R;
+  const int nbf = m0 << logW;
+  for (int b = threadIdx.x; b < nbf; b += kThreads) {
+    int w, j;
+    if (g.in_row) {
+      j = b % m0;
+      w = b / m0;
+    } else {
+      w = b & (W - 1);
+      j = b >> logW;
+    }
+    const bool valid = w < wcount;
+    const C* src = in + bin + (int64_t)w * g.sin[0];
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int n = j + r * m0;
+      C x = valid ? src[(int64_t)n * g.sn_in] : C{0, 0};
+      if (g.conj_in) x.y = -x.y;
+      if (g.tw_mode == TW_PRE) {
+        const int64_t t = (g.tw_dim == 0) ? (w0 + w) : tconst;
+        x = cmul(x, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)n * t));
+      }
+      v[r] = x;
+    }
+    dft<R>(v);
+    if (nst > 1 && j != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tb.twL[j * r]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) sm[(j + r * m0) * pitch + w] = v[r];
+  }
+}
+
+template <int R, typename C>
+__device__ __forceinline__ void stage_mid(const PassTables<C>& tb, C* sm, int L, int W, int logW,
+                                          int pitch, int span, int Ls) {
+  const int m = span / R;
+  const int nbf = (L / R) << logW;
+  for (int b = threadIdx.x; b < nbf; b += kThreads) {
+    const int w = b & (W - 1);
+    const int q = b >> logW;
+    const int blk = q / m;
+    const int j = q - blk * m;
+    const int base = blk * span + j;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = sm[(base + r * m) * pitch + w];
+    dft<R>(v);
+    if (m > 1 && j != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tb.twL[j * r * Ls]);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) sm[(base + r * m) * pitch + w] = v[r];
+  }
+}
+
+#define SHAFFT_RADIX_DISPATCH(RAD, CALL) \
+  switch (RAD) {                         \
+    case 2: CALL(2); break;              \
+    case 3: CALL(3); break;              \
+    case 4: CALL(4); break;              \
+    case 5: CALL(5); break;              \
+    case 7: CALL(7); break;              \
+    case 8: CALL(8); break;              \
+    case 11: CALL(11); break;            \
+    case 13: CALL(13); break;            \
+    case 16: CALL(16); break;            \
+    default: break;                      \
+  }
+
+__host__ __device__ constexpr int ilog2c(int x) {
+  int l = 0;
+  while ((1 << l) < x) ++l;
+  return l;
+}
+
+template <typename T, int LS, int WS>
+__global__ void __launch_bounds__(kThreads)
+    k_fft_pass(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
+               typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+  using C = typename Cx<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  constexpr RadixPlan P = radix_plan(LS > 0 ? LS : 1);
+  const int L = LS ? LS : g.L;
+  const int W = WS ? WS : g.W;
+  const int logW = WS ? ilog2c(WS) : g.logW;
+  const int pitch = WS ? (WS == 1 ? 1 : WS + 1) : g.pitch;
+  const int nst = LS ? P.n : g.nst;
+
+  for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+    int64_t rest = tile;
+    const int64_t tw = rest % g.tiles_w;
+    rest /= g.tiles_w;
+    const int64_t i1 = rest % g.ext[1];
+    rest /= g.ext[1];
+    const int64_t i2 = rest % g.ext[2];
+    const int64_t i3 = rest / g.ext[2];
+    const int64_t w0 = tw * W;
+    const int wcount = (int)((g.ext[0] - w0) < W ? (g.ext[0] - w0) : W);
+    const int64_t bin = w0 * g.sin[0] + i1 * g.sin[1] + i2 * g.sin[2] + i3 * g.sin[3];
+    const int64_t bout = w0 * g.sout[0] + i1 * g.sout[1] + i2 * g.sout[2] + i3 * g.sout[3];
+    const int64_t tconst = g.tw_dim == 1 ? i1 : (g.tw_dim == 2 ? i2 : (g.tw_dim == 3 ? i3 : 0));
+
+    // phase 1: load + first radix stage
+    {
+      const int r0 = LS ? P.r[0] : g.rad[0];
+#define SHAFFT_CALL_FIRST(R) \
+  stage_first<R, C>(g, tb, in, sm, L, W, logW, pitch, nst, wcount, bin, w0, tconst)
+      SHAFFT_RADIX_DISPATCH(r0, SHAFFT_CALL_FIRST)
+#undef SHAFFT_CALL_FIRST
+    }
+    __syncthreads();
+    // phase 2: remaining stages in shared memory
+    {
+      int span = L;
+#pragma unroll
+      for (int s = 1; s < (LS ? P.n : kMaxStages); ++s) {
+        if (!LS && s >= nst) break;
+        span /= (LS ? P.r[s - 1] : g.rad[s - 1]);
+        const int Ls = L / span;
+        const int rs = LS ? P.r[s] : g.rad[s];
+#define SHAFFT_CALL_MID(R) stage_mid<R, C>(tb, sm, L, W, logW, pitch, span, Ls)
+        SHAFFT_RADIX_DISPATCH(rs, SHAFFT_CALL_MID)
+#undef SHAFFT_CALL_MID
+        __syncthreads();
+      }
+    }
+    // phase 3: digit-reversed read, fused twiddle/scale/conj, store
+    {
+      const int total = L << logW;
+      const T scale = (T)g.scale;
+      for (int b = threadIdx.x; b < total; b += kThreads) {
+        int w, p, k;
+        if (g.out_row) {
+          k = b % L;
+          w = b / L;
+          p = tb.k2p[k];
+        } else {
+          w = b & (W - 1);
+          p = b >> logW;
+          k = tb.p2k[p];
+        }
+        if (w >= wcount) continue;
+        C x = sm[p * pitch + w];
+        if (g.tw_mode == TW_POST) {
+          const int64_t t = (g.tw_dim == 0) ? (w0 + w) : tconst;
+          x = cmul(x, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * t));
+        }
+        if (g.scale != 1.0) x = cscale(x, scale);
+        if (g.conj_out) x.y = -x.y;
+        out[bout + (int64_t)w * g.sout[0] + (int64_t)k * g.sk_out] = x;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise kernels
+// ---------------------------------------------------------------------------
+
+// data[i] = conj?(src[i]) * factor   (normalize, copies)
+template <typename T>
+__global__ void k_scale_copy(const typename Cx<T>::type* src, typename Cx<T>::type* dst, int64_t n,
+                             T factor, int conj) {
+  using C = typename Cx<T>::type;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    C x = src[i];
+    x.x *= factor;
+    x.y *= factor;
+    if (conj) x.y = -x.y;
+    dst[i] = x;
+  }
+}
+
+// Bluestein modulate: dst[b*M + m] = (m < L) ? conj?(x(o, m, i)) * chirp[m] : 0
+// with b = o*I + i and x(o, m, i) = src[(o*L + m)*I + i].
+template <typename T>
+__global__ void k_bs_modulate(const typename Cx<T>::type* src, typename Cx<T>::type* dst, int64_t L,
+                              int64_t M, int64_t I, int64_t total, const typename Cx<T>::type* chirp,
+                              int conj) {
+  using C = typename Cx<T>::type;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = idx / M, m = idx - b * M;
+    C r = C{0, 0};
+    if (m < L) {
+      const int64_t o = b / I, i = b - o * I;
+      C x = src[(o * L + m) * I + i];
+      if (conj) x.y = -x.y;
+      r = cmul(x, chirp[m]);
+    }
+    dst[idx] = r;
+  }
+}
+
+// s[idx] = conj(s[idx] * H[idx % M])   (H carries the 1/M of the inverse)
+template <typename T>
+__global__ void k_bs_mulh(typename Cx<T>::type* s, const typename Cx<T>::type* H, int64_t M,
+                          int64_t total) {
+  using C = typename Cx<T>::type;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    C y = cmul(s[idx], H[idx % M]);
+    y.y = -y.y;
+    s[idx] = y;
+  }
+}
+
+// Bluestein demodulate: dst(o, k, i) = conj?(chirp[k] * conj(s[b*M + k])) * scale
+template <typename T>
+__global__ void k_bs_demod(const typename Cx<T>::type* s, typename Cx<T>::type* dst, int64_t L,
+                           int64_t M, int64_t I, int64_t total, const typename Cx<T>::type* chirp,
+                           int conj, T scale) {
+  using C = typename Cx<T>::type;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = idx / L, k = idx - b * L;
+    const int64_t o = b / I, i = b - o * I;
+    C v = s[b * M + k];
+    v.y = -v.y;
+    C r = cmul(chirp[k], v);
+    r.x *= scale;
+    r.y *= scale;
+    if (conj) r.y = -r.y;
+    dst[(o * L + k) * I + i] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Table generation (FP64 phase, rounded once to the storage type)
+// ---------------------------------------------------------------------------
+
+// out[i] = exp(-2*pi*i * ((i*mult) mod N) / N), i < count
+template <typename T>
+__global__ void k_gen_twiddle(typename Cx<T>::type* out, int64_t count, int64_t mult, int64_t N) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t m = ((unsigned __int128)(uint64_t)i * (uint64_t)mult) % (uint64_t)N;
+    double s, c;
+    sincospi(-2.0 * ((double)m / (double)N), &s, &c);
+    out[i] = typename Cx<T>::type{(T)c, (T)s};
+  }
+}
+
+// chirp[m] = exp(-i*pi*(m^2 mod 2L)/L), m < L  (integer phase reduction)
+template <typename T>
+__global__ void k_gen_chirp(typename Cx<T>::type* out, int64_t L) {
+  for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < L;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = ((unsigned __int128)(uint64_t)m * (uint64_t)m) % (uint64_t)(2 * L);
+    double s, c;
+    sincospi(-((double)r / (double)L), &s, &c);
+    out[m] = typename Cx<T>::type{(T)c, (T)s};
+  }
+}
+
+// Bluestein kernel sequence h (length M): conj(chirp[|j|]) cyclically, zero elsewhere.
+template <typename T>
+__global__ void k_gen_bs_kernel(typename Cx<T>::type* h, const typename Cx<T>::type* chirp, int64_t L,
+                                int64_t M) {
+  using C = typename Cx<T>::type;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < M;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    C r = C{0, 0};
+    if (j < L) {
+      r = chirp[j];
+      r.y = -r.y;
+    } else if (j > M - L) {
+      r = chirp[M - j];
+      r.y = -r.y;
+    }
+    h[j] = r;
+  }
+}
+
+}  // namespace shafft_sm100

@@ -1,0 +1,122 @@
+// Pass descriptors shared by the host planner (plan.cu) and the device
+// kernels (kernels.cu).
+//
+// A "pass" is one kernel launch that reads the whole working tensor from HBM
+// once and writes it once.  It performs batched DFTs of length L (L <= 4096)
+// along one logical index "n" of a strided view of the tensor:
+//
+//   input  element (n, b0, b1, b2, b3) at  in  + n*sn_in  + sum_d b_d*sin[d]
+//   output element (k, b0, b1, b2, b3) at  out + k*sk_out + sum_d b_d*sout[d]
+//
+// b0 is the tile dimension: one CTA processes W consecutive b0 values for one
+// (b1, b2, b3) tuple, so every load/store instruction of a warp touches W
+// consecutive elements when sin[0]/sout[0] == 1 ("column" orientation) or L
+// consecutive elements when sn_in/sk_out == 1 ("row" orientation).
+//
+// Optional extras fused into the same pass:
+//   * a four-step twiddle  w_N^{(n or k) * t}  with t = b_{tw_dim} (applied to
+//     the input (PRE) or to the output (POST)); the planner guarantees the
+//     exponent is < N so no modular reduction is needed;
+//   * conjugation on input / output (backward transforms are computed as
+//     conj(F(conj(x))));
+//   * a real scale on output (fused normalisation).
+#pragma once
+#include <stdint.h>
+
+namespace shafft_sm100 {
+
+constexpr int kMaxStages = 16;
+constexpr int kMaxPassLen = 4096;
+constexpr int kThreads = 256;
+
+enum TwMode : int { TW_NONE = 0, TW_PRE = 1, TW_POST = 2 };
+
+struct RadixPlan {
+  int n = 0;
+  int r[kMaxStages] = {};
+};
+
+// Radix sequence for a pass of length L (L must factor into 2,3,5,7,11,13).
+// Powers of two are split into as many 8/16 stages as keep the stage count
+// minimal (512 = 8*8*8, 4096 = 16*16*16); odd primes follow.
+__host__ __device__ constexpr RadixPlan radix_plan(int L) {
+  RadixPlan p{};
+  int e = 0;
+  while (L % 2 == 0) {
+    L /= 2;
+    ++e;
+  }
+  int n16 = e / 4, rem = e % 4;
+  int pw[kMaxStages] = {};
+  int np = 0;
+  if (rem == 0) {
+    for (int i = 0; i < n16; ++i) pw[np++] = 16;
+  } else if (rem == 3) {
+    for (int i = 0; i < n16; ++i) pw[np++] = 16;
+    pw[np++] = 8;
+  } else if (rem == 2) {
+    if (n16 >= 1) {
+      for (int i = 0; i < n16 - 1; ++i) pw[np++] = 16;
+      pw[np++] = 8;
+      pw[np++] = 8;
+    } else {
+      pw[np++] = 4;
+    }
+  } else {  // rem == 1
+    if (n16 >= 2) {
+      for (int i = 0; i < n16 - 2; ++i) pw[np++] = 16;
+      pw[np++] = 8;
+      pw[np++] = 8;
+      pw[np++] = 8;
+    } else if (n16 == 1) {
+      pw[np++] = 8;
+      pw[np++] = 4;
+    } else {
+      pw[np++] = 2;
+    }
+  }
+  for (int i = 0; i < np; ++i) p.r[p.n++] = pw[i];
+  const int odd[5] = {3, 5, 7, 11, 13};
+  for (int oi = 0; oi < 5; ++oi)
+    while (L % odd[oi] == 0) {
+      L /= odd[oi];
+      p.r[p.n++] = odd[oi];
+    }
+  if (L != 1) p.n = -1;  // not representable
+  return p;
+}
+
+struct PassGeom {
+  int L;
+  int nst;
+  int rad[kMaxStages];
+  int W;       // tile width along b0 (power of two)
+  int logW;
+  int pitch;   // shared-memory row pitch in elements: element (p, w) at p*pitch + w
+  int in_row;  // 1: lanes walk n at load (sn_in == 1)
+  int out_row; // 1: lanes walk k at store (sk_out == 1)
+  int64_t ext[4];
+  int64_t sin[4];
+  int64_t sout[4];
+  int64_t sn_in, sk_out;
+  int64_t tiles_w;  // ceil(ext[0] / W)
+  int64_t ntiles;   // tiles_w * ext[1] * ext[2] * ext[3]
+  int tw_mode;
+  int tw_dim;
+  int tw_shift;     // two-level table split: m = (m >> shift, m & mask)
+  int64_t tw_mask;
+  int conj_in, conj_out;
+  double scale;
+};
+
+// Device pointers a pass reads besides its input/output.
+template <typename C>
+struct PassTables {
+  const C* twL;            // w_L^m, m < L
+  const uint16_t* p2k;     // digit-reversed position -> frequency index
+  const uint16_t* k2p;     // frequency index -> position
+  const C* tw_hi;          // w_N^{(m >> shift) << shift}
+  const C* tw_lo;          // w_N^{m & mask}
+};
+
+}  // namespace shafft_sm100

@@ -1,0 +1,850 @@
+// Planner, executor and C ABI of libshafft_sm100.so.
+//
+// The planner turns "C2C DFT over every axis of a row-major tensor" into a
+// list of HBM passes (see pass.h).  Per axis of length L, inner stride I and
+// outer count O:
+//   * L == 1                       -> nothing;
+//   * L smooth, fits one pass      -> one pass (row tile if I == 1, column
+//                                     tile otherwise), in place;
+//   * L smooth, too long           -> global decimation in frequency over
+//                                     2 or 3 passes: pass s does DFTs of
+//                                     length L_s at stride L/(L_0..L_s)*I and
+//                                     multiplies by w_span^{j*k}; the last pass
+//                                     undoes the digit reversal while storing
+//                                     (out of place);
+//   * L with a prime factor > 13   -> Bluestein: modulate by the chirp into
+//                                     scratch rows of power-of-two length
+//                                     M >= 2L-1, FFT_M, multiply by the
+//                                     precomputed kernel spectrum, FFT_M,
+//                                     demodulate.
+// This replaces the reference's per-axis-group hipFFT plans
+// (src/cpp/fft/hipfft_method/fftnd_method.cpp:47-61, 73-158, 162-351), its
+// gpuTT transpose path (src/cpp/fft/hipfft_method/nd/transpose_fftnd.cpp)
+// and its Bluestein executor
+// (src/cpp/fft/hipfft_method/1d/fft1d_bluestein_executor.hip:249-356).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../../include/shafft_sm100.h"
+#include "kernels.cuh"
+#include "pass.h"
+
+namespace shafft_sm100 {
+
+static thread_local int g_last_cuda = 0;
+static thread_local char g_last_msg[512] = "";
+
+static int set_err(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+static int set_err(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_msg, sizeof(g_last_msg), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      g_last_cuda = (int)e_;                                                             \
+      return set_err(SHAFFT_SM100_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), \
+                     __FILE__, __LINE__);                                                \
+    }                                                                                    \
+  } while (0)
+
+enum StepKind : int { ST_PASS = 0, ST_BS_MOD, ST_BS_MULH, ST_BS_DEMOD, ST_COPY };
+enum BufId : int { BUF_SRC = 0, BUF_DST = 1, BUF_S0 = 2, BUF_S1 = 3 };
+
+static int other_buf(int b) {
+  switch (b) {
+    case BUF_SRC: return BUF_DST;
+    case BUF_DST: return BUF_SRC;
+    case BUF_S0: return BUF_S1;
+    default: return BUF_S0;
+  }
+}
+
+static const char* buf_name(int b) {
+  static const char* n[] = {"src", "dst", "s0", "s1"};
+  return n[b & 3];
+}
+
+struct Step {
+  int kind = ST_PASS;
+  PassGeom g{};
+  int in_buf = BUF_SRC, out_buf = BUF_DST;
+  int tabL = -1, tabN = -1, tabB = -1;
+  int64_t bsL = 0, bsM = 0, bsI = 1, total = 0;
+  size_t smem = 0;
+};
+
+struct LTable {
+  int L;
+  size_t off_tw, off_p2k, off_k2p;
+};
+struct NTable {
+  int64_t N;
+  int shift;
+  int64_t mask, nhi, nlo;
+  size_t off_hi, off_lo;
+};
+struct BTable {
+  int64_t L, M;
+  size_t off_chirp, off_H;
+  std::vector<Step> hsteps;  // FFT_M of the kernel sequence (S0 -> result buf)
+  int hresult_buf;
+};
+
+struct Limits {
+  int max_row;   // longest row-tile pass
+  int max_col;   // longest column-tile pass
+  int e_target;  // tile elements aimed at (64 KiB of complex data)
+  int w_col;     // widest column tile
+};
+
+static Limits limits_for(int precision) {
+  if (precision == 0) return Limits{4096, 2048, 8192, 16};
+  return Limits{4096, 2048, 4096, 8};
+}
+
+static bool is_smooth(int64_t L) {
+  const int64_t primes[] = {2, 3, 5, 7, 11, 13};
+  for (int64_t p : primes)
+    while (L % p == 0) L /= p;
+  return L == 1;
+}
+
+static int pow2floor(int64_t x) {
+  int p = 1;
+  while ((int64_t)p * 2 <= x && p < (1 << 30)) p *= 2;
+  return p;
+}
+static int pow2ceil(int64_t x) {
+  int p = 1;
+  while (p < x && p < (1 << 30)) p *= 2;
+  return p;
+}
+
+struct Planner {
+  int precision;
+  Limits lim;
+  size_t elem;
+  std::vector<LTable> ltabs;
+  std::vector<NTable> ntabs;
+  std::vector<BTable> btabs;
+  size_t table_bytes = 0;
+  int64_t scratch_elems = 0;
+
+  explicit Planner(int prec) : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {}
+
+  size_t alloc(size_t bytes) {
+    size_t off = (table_bytes + 255) & ~size_t(255);
+    table_bytes = off + bytes;
+    return off;
+  }
+
+  int ltab(int L) {
+    for (size_t i = 0; i < ltabs.size(); ++i)
+      if (ltabs[i].L == L) return (int)i;
+    LTable t;
+    t.L = L;
+    t.off_tw = alloc(elem * L);
+    t.off_p2k = alloc(2 * L);
+    t.off_k2p = alloc(2 * L);
+    ltabs.push_back(t);
+    return (int)ltabs.size() - 1;
+  }
+
+  int ntab(int64_t N) {
+    for (size_t i = 0; i < ntabs.size(); ++i)
+      if (ntabs[i].N == N) return (int)i;
+    NTable t;
+    t.N = N;
+    int lg = 0;
+    while ((int64_t(1) << lg) < N) ++lg;
+    t.shift = (lg + 1) / 2;
+    t.mask = (int64_t(1) << t.shift) - 1;
+    t.nlo = int64_t(1) << t.shift;
+    t.nhi = (N + t.nlo - 1) / t.nlo + 1;
+    t.off_hi = alloc(elem * t.nhi);
+    t.off_lo = alloc(elem * t.nlo);
+    ntabs.push_back(t);
+    return (int)ntabs.size() - 1;
+  }
+
+  void fill_radix(PassGeom& g, int L) {
+    RadixPlan rp = radix_plan(L);
+    g.L = L;
+    g.nst = rp.n;
+    for (int s = 0; s < rp.n; ++s) g.rad[s] = rp.r[s];
+  }
+
+  void finish_geom(Step& st, int W) {
+    PassGeom& g = st.g;
+    g.W = W;
+    g.logW = 0;
+    while ((1 << g.logW) < W) ++g.logW;
+    g.pitch = (W == 1) ? 1 : W + 1;
+    for (int d = 0; d < 4; ++d)
+      if (g.ext[d] < 1) g.ext[d] = 1;
+    g.tiles_w = (g.ext[0] + W - 1) / W;
+    g.ntiles = g.tiles_w * g.ext[1] * g.ext[2] * g.ext[3];
+    g.in_row = (g.sn_in == 1) ? 1 : 0;
+    g.out_row = (g.sk_out == 1) ? 1 : 0;
+    g.scale = 1.0;
+    st.smem = (size_t)g.L * (size_t)g.pitch * elem;
+    st.tabL = ltab(g.L);
+  }
+
+  int col_width(int L, int64_t I) const {
+    int w = lim.e_target / L;
+    if (w < 1) w = 1;
+    w = std::min(w, lim.w_col);
+    w = pow2floor(w);
+    w = std::min(w, pow2ceil(I));
+    return std::max(w, 1);
+  }
+
+  // one pass over axis (O, L, I): in_buf -> out_buf (may be equal)
+  void single_pass(std::vector<Step>& out, int64_t O, int L, int64_t I, int in_buf, int out_buf) {
+    Step st;
+    st.kind = ST_PASS;
+    st.in_buf = in_buf;
+    st.out_buf = out_buf;
+    fill_radix(st.g, L);
+    PassGeom& g = st.g;
+    if (I == 1) {
+      int W = pow2floor(std::max<int64_t>(1, std::min<int64_t>(O, lim.e_target / L)));
+      W = std::min(W, 32);
+      g.ext[0] = O;
+      g.sin[0] = g.sout[0] = L;
+      g.ext[1] = g.ext[2] = g.ext[3] = 1;
+      g.sn_in = g.sk_out = 1;
+      finish_geom(st, W);
+    } else {
+      int W = col_width(L, I);
+      g.ext[0] = I;
+      g.sin[0] = g.sout[0] = 1;
+      g.ext[1] = O;
+      g.sin[1] = g.sout[1] = (int64_t)L * I;
+      g.ext[2] = g.ext[3] = 1;
+      g.sn_in = g.sk_out = I;
+      finish_geom(st, W);
+    }
+    out.push_back(st);
+  }
+
+  // choose 2- or 3-factor split of a smooth L; returns empty if impossible
+  std::vector<int> split(int64_t L, int64_t I) const {
+    const int max_last = (I == 1) ? lim.max_row : lim.max_col;
+    std::vector<int> best;
+    // 2 factors: largest last factor whose cofactor fits a column pass
+    for (int64_t d = std::min<int64_t>(L, max_last); d >= 2; --d) {
+      if (L % d) continue;
+      int64_t c = L / d;
+      if (c <= lim.max_col && c >= 2) {
+        best = {(int)c, (int)d};
+        break;
+      }
+    }
+    if (!best.empty()) return best;
+    for (int64_t d = std::min<int64_t>(L, max_last); d >= 2; --d) {
+      if (L % d) continue;
+      int64_t c = L / d;
+      // split c into two column factors as balanced as possible
+      int64_t bestf = -1;
+      for (int64_t f = 2; f * f <= c; ++f)
+        if (c % f == 0 && f <= lim.max_col && c / f <= lim.max_col) bestf = f;
+      if (bestf > 0) return {(int)(c / bestf), (int)bestf, (int)d};
+    }
+    return {};
+  }
+
+  // global decimation-in-frequency over the factors Ls
+  void multi_pass(std::vector<Step>& out, int64_t O, int64_t L, int64_t I, const std::vector<int>& Ls,
+                  int in_buf, int out_buf) {
+    const int S = (int)Ls.size();
+    int64_t span = L;
+    // in-place passes
+    for (int s = 0; s < S - 1; ++s) {
+      const int R = Ls[s];
+      const int64_t m = span / R;
+      Step st;
+      st.kind = ST_PASS;
+      st.in_buf = (s == 0) ? in_buf : out_buf;
+      st.out_buf = out_buf;
+      fill_radix(st.g, R);
+      PassGeom& g = st.g;
+      g.sn_in = g.sk_out = m * I;
+      int W;
+      if (I > 1) {
+        g.ext[0] = I;  g.sin[0] = g.sout[0] = 1;
+        g.ext[1] = m;  g.sin[1] = g.sout[1] = I;
+        g.ext[2] = L / span;  g.sin[2] = g.sout[2] = span * I;
+        g.ext[3] = O;  g.sin[3] = g.sout[3] = L * I;
+        g.tw_dim = 1;
+        W = col_width(R, I);
+      } else {
+        g.ext[0] = m;  g.sin[0] = g.sout[0] = 1;
+        g.ext[1] = L / span;  g.sin[1] = g.sout[1] = span;
+        g.ext[2] = O;  g.sin[2] = g.sout[2] = L;
+        g.ext[3] = 1;  g.sin[3] = g.sout[3] = 0;
+        g.tw_dim = 0;
+        W = col_width(R, m);
+      }
+      g.tw_mode = TW_POST;
+      st.tabN = ntab(span);
+      finish_geom(st, W);
+      out.push_back(st);
+      span = m;
+    }
+    // last pass: undo digit reversal while storing
+    {
+      const int R = Ls[S - 1];
+      Step st;
+      st.kind = ST_PASS;
+      st.in_buf = (S == 1) ? in_buf : out_buf;
+      st.out_buf = other_buf(st.in_buf);
+      fill_radix(st.g, R);
+      PassGeom& g = st.g;
+      g.sn_in = I;
+      g.sk_out = (L / R) * I;
+      // digit t: input stride m_t*I, output stride (L_0..L_{t-1})*I
+      int64_t din[2] = {0, 0}, dout[2] = {0, 0}, dext[2] = {1, 1};
+      int64_t prod = 1;
+      for (int t = 0; t < S - 1; ++t) {
+        prod *= Ls[t];
+        dext[t] = Ls[t];
+        din[t] = (L / prod) * I;
+        dout[t] = (prod / Ls[t]) * I;
+      }
+      int W;
+      if (I > 1) {
+        g.ext[0] = I;  g.sin[0] = g.sout[0] = 1;
+        g.ext[1] = dext[0];  g.sin[1] = din[0];  g.sout[1] = dout[0];
+        g.ext[2] = dext[1];  g.sin[2] = din[1];  g.sout[2] = dout[1];
+        g.ext[3] = O;  g.sin[3] = g.sout[3] = L * I;
+        W = col_width(R, I);
+      } else {
+        g.ext[0] = dext[0];  g.sin[0] = din[0];  g.sout[0] = dout[0];
+        g.ext[1] = dext[1];  g.sin[1] = din[1];  g.sout[1] = dout[1];
+        g.ext[2] = O;  g.sin[2] = g.sout[2] = L;
+        g.ext[3] = 1;  g.sin[3] = g.sout[3] = 0;
+        // row tile in, column tile out: W rows of R contiguous inputs
+        W = pow2floor(std::max<int64_t>(1, std::min<int64_t>(dext[0], lim.e_target / R)));
+        W = std::min(W, lim.w_col);
+      }
+      finish_geom(st, W);
+      out.push_back(st);
+    }
+  }
+
+  int btab(int64_t L, int64_t M) {
+    for (size_t i = 0; i < btabs.size(); ++i)
+      if (btabs[i].L == L && btabs[i].M == M) return (int)i;
+    BTable t;
+    t.L = L;
+    t.M = M;
+    t.off_chirp = alloc(elem * L);
+    t.off_H = alloc(elem * M);
+    scratch_elems = std::max(scratch_elems, M);
+    // the kernel spectrum FFT_M(h): plan it on scratch S0 -> ...
+    int cur = BUF_S0;
+    int rc = axis(t.hsteps, 1, M, 1, cur, false, /*in_bluestein=*/true);
+    (void)rc;
+    t.hresult_buf = cur;
+    btabs.push_back(t);
+    return (int)btabs.size() - 1;
+  }
+
+  // Plan one axis; `cur` holds the data on entry and on exit.
+  int axis(std::vector<Step>& out, int64_t O, int64_t L, int64_t I, int& cur, bool force_oop,
+           bool in_bluestein) {
+    if (L == 1) return 0;
+    const int max_one = (I == 1) ? lim.max_row : lim.max_col;
+    if (is_smooth(L) && L <= max_one) {
+      int ob = force_oop ? other_buf(cur) : cur;
+      single_pass(out, O, (int)L, I, cur, ob);
+      cur = ob;
+      return 0;
+    }
+    if (is_smooth(L)) {
+      std::vector<int> f = split(L, I);
+      if (!f.empty()) {
+        // the last pass is out of place: it lands in other(x) where x is the
+        // buffer the in-place passes used
+        const int x = force_oop ? other_buf(cur) : cur;
+        multi_pass(out, O, L, I, f, cur, x);
+        cur = out.back().out_buf;
+        return 0;
+      }
+    }
+    if (in_bluestein) return SHAFFT_SM100_ENOTSUP;
+    // Bluestein
+    int64_t M = 1;
+    while (M < 2 * L - 1) M <<= 1;
+    const int64_t B = O * I;
+    const int bt = btab(L, M);
+    scratch_elems = std::max(scratch_elems, B * M);
+    Step mod;
+    mod.kind = ST_BS_MOD;
+    mod.in_buf = cur;
+    mod.out_buf = BUF_S0;
+    mod.tabB = bt;
+    mod.bsL = L;
+    mod.bsM = M;
+    mod.bsI = I;
+    mod.total = B * M;
+    out.push_back(mod);
+    int sc = BUF_S0;
+    int rc = axis(out, B, M, 1, sc, false, true);
+    if (rc) return rc;
+    Step mul;
+    mul.kind = ST_BS_MULH;
+    mul.in_buf = mul.out_buf = sc;
+    mul.tabB = bt;
+    mul.bsM = M;
+    mul.total = B * M;
+    out.push_back(mul);
+    rc = axis(out, B, M, 1, sc, false, true);
+    if (rc) return rc;
+    Step dem;
+    dem.kind = ST_BS_DEMOD;
+    dem.in_buf = sc;
+    dem.out_buf = force_oop ? other_buf(cur) : cur;
+    dem.tabB = bt;
+    dem.bsL = L;
+    dem.bsM = M;
+    dem.bsI = I;
+    dem.total = B * L;
+    out.push_back(dem);
+    cur = dem.out_buf;
+    return 0;
+  }
+
+  int plan_nd(std::vector<Step>& out, int ndim, const int64_t* dims) {
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      out.clear();
+      int cur = BUF_SRC;
+      bool first = true;
+      for (int a = ndim - 1; a >= 0; --a) {
+        int64_t I = 1, O = 1;
+        for (int b = a + 1; b < ndim; ++b) I *= dims[b];
+        for (int b = 0; b < a; ++b) O *= dims[b];
+        if (dims[a] == 1) continue;
+        const bool foop = first && attempt == 1;
+        int rc = axis(out, O, dims[a], I, cur, foop, false);
+        if (rc) return rc;
+        first = false;
+      }
+      if (out.empty()) {
+        Step cp;
+        cp.kind = ST_COPY;
+        cp.in_buf = BUF_SRC;
+        cp.out_buf = BUF_DST;
+        int64_t t = 1;
+        for (int b = 0; b < ndim; ++b) t *= dims[b];
+        cp.total = t;
+        out.push_back(cp);
+        return 0;
+      }
+      if (cur == BUF_DST) return 0;
+    }
+    return set_err(SHAFFT_SM100_ENOTSUP, "planner could not place the result in dst");
+  }
+};
+
+static void digit_tables(int L, std::vector<uint16_t>& p2k, std::vector<uint16_t>& k2p) {
+  RadixPlan rp = radix_plan(L);
+  p2k.assign(L, 0);
+  k2p.assign(L, 0);
+  for (int p = 0; p < L; ++p) {
+    // p = sum_s d_s * m_s with m_s = L / (r_0 .. r_s); k = sum_s d_s * (r_0..r_{s-1})
+    int rem = p, k = 0, pre = 1, span = L;
+    for (int s = 0; s < rp.n; ++s) {
+      const int m = span / rp.r[s];
+      const int d = rem / m;
+      rem -= d * m;
+      k += d * pre;
+      pre *= rp.r[s];
+      span = m;
+    }
+    p2k[p] = (uint16_t)k;
+    k2p[k] = (uint16_t)p;
+  }
+}
+
+}  // namespace shafft_sm100
+
+using namespace shafft_sm100;
+
+struct shafft_sm100_plan_s {
+  int precision = 0;
+  int ndim = 0;
+  std::vector<int64_t> dims;
+  int64_t total = 0;
+  std::vector<Step> steps;
+  std::vector<LTable> ltabs;
+  std::vector<NTable> ntabs;
+  std::vector<BTable> btabs;
+  size_t table_bytes = 0;
+  unsigned char* d_tables = nullptr;
+  int64_t scratch_elems = 0;
+  void* d_s0 = nullptr;
+  void* d_s1 = nullptr;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+};
+
+namespace {
+
+template <typename T>
+struct Launcher {
+  using C = typename Cx<T>::type;
+
+  static int set_smem_attrs() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+      err = cudaFuncSetAttribute(k_fft_pass<T, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 200 * 1024);
+    });
+    if (err != cudaSuccess) {
+      g_last_cuda = (int)err;
+      return set_err(SHAFFT_SM100_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(err));
+    }
+    return 0;
+  }
+
+  static PassTables<C> tables(const shafft_sm100_plan_s* p, const Step& st) {
+    PassTables<C> tb{};
+    const LTable& lt = p->ltabs[st.tabL];
+    tb.twL = reinterpret_cast<const C*>(p->d_tables + lt.off_tw);
+    tb.p2k = reinterpret_cast<const uint16_t*>(p->d_tables + lt.off_p2k);
+    tb.k2p = reinterpret_cast<const uint16_t*>(p->d_tables + lt.off_k2p);
+    if (st.tabN >= 0) {
+      const NTable& nt = p->ntabs[st.tabN];
+      tb.tw_hi = reinterpret_cast<const C*>(p->d_tables + nt.off_hi);
+      tb.tw_lo = reinterpret_cast<const C*>(p->d_tables + nt.off_lo);
+    }
+    return tb;
+  }
+
+  static int pass(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* out,
+                  bool conj_in, bool conj_out, double scale, cudaStream_t s) {
+    int rc = set_smem_attrs();
+    if (rc) return rc;
+    PassGeom g = st.g;
+    g.conj_in = conj_in;
+    g.conj_out = conj_out;
+    g.scale = scale;
+    if (st.tabN >= 0) {
+      const NTable& nt = p->ntabs[st.tabN];
+      g.tw_shift = nt.shift;
+      g.tw_mask = nt.mask;
+    }
+    PassTables<C> tb = tables(p, st);
+    int64_t grid = std::min<int64_t>(g.ntiles, 148 * 64);
+    k_fft_pass<T, 0, 0><<<(unsigned)grid, kThreads, st.smem, s>>>(
+        g, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), tb);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+  }
+
+  static unsigned grid_for(int64_t n) {
+    int64_t g = (n + 255) / 256;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+  }
+
+  static int elementwise(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* out,
+                         bool conj_in, bool conj_out, double scale, cudaStream_t s) {
+    const C* cin = reinterpret_cast<const C*>(in);
+    C* cout = reinterpret_cast<C*>(out);
+    if (st.kind == ST_COPY) {
+      k_scale_copy<T><<<grid_for(st.total), 256, 0, s>>>(cin, cout, st.total, (T)scale,
+                                                        (conj_in != conj_out) ? 1 : 0);
+    } else {
+      const BTable& bt = p->btabs[st.tabB];
+      const C* chirp = reinterpret_cast<const C*>(p->d_tables + bt.off_chirp);
+      const C* H = reinterpret_cast<const C*>(p->d_tables + bt.off_H);
+      if (st.kind == ST_BS_MOD) {
+        k_bs_modulate<T><<<grid_for(st.total), 256, 0, s>>>(cin, cout, st.bsL, st.bsM, st.bsI,
+                                                           st.total, chirp, conj_in ? 1 : 0);
+      } else if (st.kind == ST_BS_MULH) {
+        k_bs_mulh<T><<<grid_for(st.total), 256, 0, s>>>(cout, H, st.bsM, st.total);
+      } else {
+        k_bs_demod<T><<<grid_for(st.total), 256, 0, s>>>(cin, cout, st.bsL, st.bsM, st.bsI, st.total,
+                                                        chirp, conj_out ? 1 : 0, (T)scale);
+      }
+    }
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+  }
+
+  static int run_steps(const shafft_sm100_plan_s* p, const std::vector<Step>& steps, void* const bufs[4],
+                       bool conj, double scale, cudaStream_t s) {
+    const size_t n = steps.size();
+    for (size_t i = 0; i < n; ++i) {
+      const Step& st = steps[i];
+      const bool first = (i == 0), last = (i + 1 == n);
+      const bool cin = first && conj;
+      const bool cout = last && conj;
+      const double sc = last ? scale : 1.0;
+      int rc;
+      if (st.kind == ST_PASS)
+        rc = pass(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
+      else
+        rc = elementwise(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
+      if (rc) return rc;
+    }
+    return 0;
+  }
+
+  // Build every table of the plan on the device.
+  static int build_tables(shafft_sm100_plan_s* p) {
+    for (const LTable& lt : p->ltabs) {
+      k_gen_twiddle<T><<<grid_for(lt.L), 256, 0, p->stream>>>(
+          reinterpret_cast<C*>(p->d_tables + lt.off_tw), lt.L, 1, lt.L);
+      CUDA_TRY(cudaGetLastError());
+      std::vector<uint16_t> p2k, k2p;
+      digit_tables(lt.L, p2k, k2p);
+      CUDA_TRY(cudaMemcpyAsync(p->d_tables + lt.off_p2k, p2k.data(), 2 * lt.L,
+                               cudaMemcpyHostToDevice, p->stream));
+      CUDA_TRY(cudaMemcpyAsync(p->d_tables + lt.off_k2p, k2p.data(), 2 * lt.L,
+                               cudaMemcpyHostToDevice, p->stream));
+      CUDA_TRY(cudaStreamSynchronize(p->stream));
+    }
+    for (const NTable& nt : p->ntabs) {
+      k_gen_twiddle<T><<<grid_for(nt.nhi), 256, 0, p->stream>>>(
+          reinterpret_cast<C*>(p->d_tables + nt.off_hi), nt.nhi, nt.nlo, nt.N);
+      k_gen_twiddle<T><<<grid_for(nt.nlo), 256, 0, p->stream>>>(
+          reinterpret_cast<C*>(p->d_tables + nt.off_lo), nt.nlo, 1, nt.N);
+      CUDA_TRY(cudaGetLastError());
+    }
+    for (const BTable& bt : p->btabs) {
+      C* chirp = reinterpret_cast<C*>(p->d_tables + bt.off_chirp);
+      k_gen_chirp<T><<<grid_for(bt.L), 256, 0, p->stream>>>(chirp, bt.L);
+      k_gen_bs_kernel<T><<<grid_for(bt.M), 256, 0, p->stream>>>(reinterpret_cast<C*>(p->d_s0),
+                                                               chirp, bt.L, bt.M);
+      CUDA_TRY(cudaGetLastError());
+      void* bufs[4] = {nullptr, nullptr, p->d_s0, p->d_s1};
+      int rc = run_steps(p, bt.hsteps, bufs, false, 1.0 / (double)bt.M, p->stream);
+      if (rc) return rc;
+      CUDA_TRY(cudaMemcpyAsync(p->d_tables + bt.off_H, bufs[bt.hresult_buf], sizeof(C) * bt.M,
+                               cudaMemcpyDeviceToDevice, p->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(p->stream));
+    return 0;
+  }
+};
+
+std::string describe_steps(int precision, const std::vector<Step>& steps, int64_t total) {
+  std::string s = "{\"precision\":" + std::to_string(precision) + ",\"elements\":" +
+                  std::to_string(total) + ",\"steps\":[";
+  for (size_t i = 0; i < steps.size(); ++i) {
+    const Step& st = steps[i];
+    char b[768];
+    if (st.kind == ST_PASS) {
+      std::string rad;
+      for (int r = 0; r < st.g.nst; ++r) rad += (r ? "," : "") + std::to_string(st.g.rad[r]);
+      snprintf(b, sizeof(b),
+               "{\"kind\":\"pass\",\"L\":%d,\"radices\":[%s],\"W\":%d,\"in\":\"%s\",\"out\":\"%s\","
+               "\"in_row\":%d,\"out_row\":%d,\"tiles\":%lld,\"smem\":%zu,\"twiddle\":%d,"
+               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld}",
+               st.g.L, rad.c_str(), st.g.W, buf_name(st.in_buf), buf_name(st.out_buf), st.g.in_row,
+               st.g.out_row, (long long)st.g.ntiles, st.smem, st.g.tw_mode, (long long)st.g.ext[0],
+               (long long)st.g.ext[1], (long long)st.g.ext[2], (long long)st.g.ext[3],
+               (long long)st.g.sn_in, (long long)st.g.sk_out);
+    } else {
+      const char* k = st.kind == ST_BS_MOD    ? "bluestein_modulate"
+                      : st.kind == ST_BS_MULH ? "bluestein_multiply"
+                      : st.kind == ST_BS_DEMOD ? "bluestein_demodulate"
+                                               : "copy";
+      snprintf(b, sizeof(b), "{\"kind\":\"%s\",\"L\":%lld,\"M\":%lld,\"in\":\"%s\",\"out\":\"%s\",\"total\":%lld}",
+               k, (long long)st.bsL, (long long)st.bsM, buf_name(st.in_buf), buf_name(st.out_buf),
+               (long long)st.total);
+    }
+    if (i) s += ",";
+    s += b;
+  }
+  s += "]}";
+  return s;
+}
+
+int copy_out(const std::string& s, char* buf, int buflen) {
+  if (!buf || buflen <= 0) return SHAFFT_SM100_EINVAL;
+  if ((int)s.size() + 1 > buflen) {
+    memcpy(buf, s.data(), buflen - 1);
+    buf[buflen - 1] = 0;
+    return set_err(SHAFFT_SM100_EINVAL, "description truncated (%zu bytes needed)", s.size() + 1);
+  }
+  memcpy(buf, s.c_str(), s.size() + 1);
+  return 0;
+}
+
+int validate_dims(int ndim, const int64_t* dims, int precision, int64_t* total) {
+  if (ndim < 1 || ndim > 64 || !dims) return set_err(SHAFFT_SM100_EINVAL, "bad ndim/dims");
+  if (precision != 0 && precision != 1) return set_err(SHAFFT_SM100_EINVAL, "bad precision");
+  int64_t t = 1;
+  for (int a = 0; a < ndim; ++a) {
+    if (dims[a] < 1) return set_err(SHAFFT_SM100_EINVAL, "dims[%d] = %lld < 1", a, (long long)dims[a]);
+    if (t > (int64_t(1) << 42) / dims[a]) return set_err(SHAFFT_SM100_ENOTSUP, "tensor too large");
+    t *= dims[a];
+  }
+  *total = t;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* buf, int buflen) {
+  int64_t total = 0;
+  int rc = validate_dims(ndim, dims, precision, &total);
+  if (rc) return rc;
+  Planner pl(precision);
+  std::vector<Step> steps;
+  rc = pl.plan_nd(steps, ndim, dims);
+  if (rc) return rc;
+  return copy_out(describe_steps(precision, steps, total), buf, buflen);
+}
+
+int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t* dims, int precision) {
+  if (!out) return set_err(SHAFFT_SM100_EINVAL, "null plan pointer");
+  *out = nullptr;
+  int64_t total = 0;
+  int rc = validate_dims(ndim, dims, precision, &total);
+  if (rc) return rc;
+  std::unique_ptr<shafft_sm100_plan_s> p(new (std::nothrow) shafft_sm100_plan_s());
+  if (!p) return set_err(SHAFFT_SM100_EALLOC, "host allocation failed");
+  p->precision = precision;
+  p->ndim = ndim;
+  p->dims.assign(dims, dims + ndim);
+  p->total = total;
+  Planner pl(precision);
+  rc = pl.plan_nd(p->steps, ndim, dims);
+  if (rc) return rc;
+  p->ltabs = pl.ltabs;
+  p->ntabs = pl.ntabs;
+  p->btabs = pl.btabs;
+  p->table_bytes = std::max<size_t>(pl.table_bytes, 256);
+  p->scratch_elems = pl.scratch_elems;
+  CUDA_TRY(cudaGetDevice(&p->device));
+  if (cudaMalloc(&p->d_tables, p->table_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for tables failed", p->table_bytes);
+  }
+  if (p->scratch_elems > 0) {
+    const size_t b = (size_t)p->scratch_elems * (precision ? 16 : 8);
+    if (cudaMalloc(&p->d_s0, b) != cudaSuccess || cudaMalloc(&p->d_s1, b) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(p->d_tables);
+      if (p->d_s0) cudaFree(p->d_s0);
+      return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for scratch failed", b);
+    }
+  }
+  rc = precision ? Launcher<double>::build_tables(p.get()) : Launcher<float>::build_tables(p.get());
+  if (rc) {
+    cudaFree(p->d_tables);
+    if (p->d_s0) cudaFree(p->d_s0);
+    if (p->d_s1) cudaFree(p->d_s1);
+    return rc;
+  }
+  *out = p.release();
+  return 0;
+}
+
+int shafft_sm100_plan_create_1d(shafft_sm100_plan* out, int64_t n, int precision) {
+  return shafft_sm100_plan_create_nd(out, 1, &n, precision);
+}
+
+int shafft_sm100_plan_destroy(shafft_sm100_plan plan) {
+  if (!plan) return 0;
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != plan->device) cudaSetDevice(plan->device);
+  if (plan->d_tables) cudaFree(plan->d_tables);
+  if (plan->d_s0) cudaFree(plan->d_s0);
+  if (plan->d_s1) cudaFree(plan->d_s1);
+  if (dev >= 0 && dev != plan->device) cudaSetDevice(dev);
+  delete plan;
+  return 0;
+}
+
+int shafft_sm100_set_stream(shafft_sm100_plan plan, void* stream) {
+  if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
+  plan->stream = reinterpret_cast<cudaStream_t>(stream);
+  return 0;
+}
+
+int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direction, double scale,
+                         void* stream) {
+  if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
+  if (!src || !dst) return set_err(SHAFFT_SM100_EINVAL, "null buffer");
+  if (src == dst) return set_err(SHAFFT_SM100_EINVAL, "src and dst must be distinct buffers");
+  if (direction != 0 && direction != 1) return set_err(SHAFFT_SM100_EINVAL, "bad direction");
+  cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : plan->stream;
+  void* bufs[4] = {src, dst, plan->d_s0, plan->d_s1};
+  return plan->precision
+             ? Launcher<double>::run_steps(plan, plan->steps, bufs, direction == 1, scale, s)
+             : Launcher<float>::run_steps(plan, plan->steps, bufs, direction == 1, scale, s);
+}
+
+int shafft_sm100_scale(void* data, size_t count, int precision, double factor, void* stream) {
+  if (!data && count) return set_err(SHAFFT_SM100_EINVAL, "null buffer");
+  if (precision != 0 && precision != 1) return set_err(SHAFFT_SM100_EINVAL, "bad precision");
+  if (count == 0) return 0;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int64_t n = (int64_t)count;
+  unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32));
+  if (precision) {
+    k_scale_copy<double><<<grid, 256, 0, s>>>(reinterpret_cast<const double2*>(data),
+                                               reinterpret_cast<double2*>(data), n, factor, 0);
+  } else {
+    k_scale_copy<float><<<grid, 256, 0, s>>>(reinterpret_cast<const float2*>(data),
+                                              reinterpret_cast<float2*>(data), n, (float)factor, 0);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int64_t shafft_sm100_plan_elements(shafft_sm100_plan plan) { return plan ? plan->total : 0; }
+
+int shafft_sm100_plan_passes(shafft_sm100_plan plan) {
+  if (!plan) return 0;
+  int n = 0;
+  for (const Step& st : plan->steps) n += (st.kind == ST_COPY) ? 1 : 1;
+  return n;
+}
+
+int shafft_sm100_plan_launches(shafft_sm100_plan plan) { return plan ? (int)plan->steps.size() : 0; }
+
+size_t shafft_sm100_plan_device_bytes(shafft_sm100_plan plan) {
+  if (!plan) return 0;
+  return plan->table_bytes + 2 * (size_t)plan->scratch_elems * (plan->precision ? 16 : 8);
+}
+
+int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen) {
+  if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
+  return copy_out(describe_steps(plan->precision, plan->steps, plan->total), buf, buflen);
+}
+
+int shafft_sm100_last_cuda_error(void) { return g_last_cuda; }
+
+const char* shafft_sm100_last_error_message(void) { return g_last_msg; }
+
+const char* shafft_sm100_version(void) { return "shafft-sm100 0.1.0 (sm_100a)"; }
+
+}  // extern "C"
