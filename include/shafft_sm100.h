@@ -89,8 +89,34 @@ size_t shafft_sm100_plan_device_bytes(shafft_sm100_plan plan);
  * the pass list for the given shape into buf.  Returns the status code. */
 int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* buf, int buflen);
 
+/* Run only step `step` (0 <= step < plan_launches()) of an execute with the
+ * same buffer roles as shafft_sm100_execute.  Running steps 0..n-1 in order
+ * on one stream is exactly one execute; used to time each kernel with
+ * events placed between the launches. */
+int shafft_sm100_execute_step(shafft_sm100_plan plan, int step, void* src, void* dst, int direction,
+                              double scale, void* stream);
+
+/* Algorithmic HBM bytes of step `step` (one compulsory read and write of
+ * what the kernel touches), or 0 for an invalid step. */
+int64_t shafft_sm100_step_bytes(shafft_sm100_plan plan, int step);
+
 /* JSON description of a created plan. */
 int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen);
+
+/* Device memory and stream helpers, so that callers above this ABI need no
+ * CUDA runtime of their own (they replace the reference's allocBufferT /
+ * freeBufferT / copyToBufferT / copyFromBufferT,
+ * src/cpp/detail/buffer_utils.hpp:36-127, and its hipStreamSynchronize). */
+#define SHAFFT_SM100_H2D 1
+#define SHAFFT_SM100_D2H 2
+#define SHAFFT_SM100_D2D 3
+int shafft_sm100_malloc(void** ptr, size_t bytes);
+int shafft_sm100_free(void* ptr);
+/* stream == NULL: synchronous copy; otherwise asynchronous on that stream. */
+int shafft_sm100_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);
+int shafft_sm100_stream_sync(void* stream);
+/* Name of the current CUDA device. */
+int shafft_sm100_device_name(char* buf, int buflen);
 
 /* Last CUDA runtime error code seen by this library on this thread. */
 int shafft_sm100_last_cuda_error(void);

@@ -146,14 +146,17 @@ def plane_waves(shape, nwaves: int = 8, seed: int = 42):
     """Sum of seeded plane waves a_j * exp(+2 pi i k_j . x / n) with integer
     wavevectors; returns (field, list of (k, a))."""
     rng = np.random.Generator(np.random.MT19937(seed + 1))
-    grids = np.meshgrid(*[np.arange(n) for n in shape], indexing="ij")
     field = np.zeros(shape, dtype=np.complex128)
     waves = []
     for _ in range(nwaves):
         k = tuple(int(rng.integers(0, n)) for n in shape)
         a = float(rng.uniform(0.5, 1.0))
-        phase = sum(ki * g / n for ki, g, n in zip(k, grids, shape))
-        field += a * np.exp(2j * np.pi * phase)
+        # separable: prod_d exp(2 pi i k_d x_d / n_d), phases reduced exactly
+        term = np.array(a, dtype=np.complex128)
+        for ki, n in zip(k, shape):
+            e = np.exp(2j * np.pi * ((ki * np.arange(n)) % n) / n)
+            term = np.multiply.outer(term, e)
+        field += term
         waves.append((k, a))
     return field, waves
 

@@ -48,6 +48,9 @@ def load():
     lib.shafft_sm100_plan_query.argtypes = [ctypes.c_int, i64p, ctypes.c_int, ctypes.c_char_p,
                                             ctypes.c_int]
     lib.shafft_sm100_plan_describe.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    lib.shafft_sm100_execute_step.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double, vp]
+    lib.shafft_sm100_step_bytes.argtypes = [vp, ctypes.c_int]
+    lib.shafft_sm100_step_bytes.restype = ctypes.c_int64
     lib.shafft_sm100_last_error_message.restype = ctypes.c_char_p
     lib.shafft_sm100_version.restype = ctypes.c_char_p
     _lib = lib
@@ -88,6 +91,16 @@ class Plan:
         _check(self._lib.shafft_sm100_execute(self.handle, ctypes.c_void_p(src_ptr),
                                               ctypes.c_void_p(dst_ptr), int(direction),
                                               float(scale), ctypes.c_void_p(stream)), "execute")
+
+    def execute_step(self, step: int, src_ptr: int, dst_ptr: int, direction: int = 0,
+                     scale: float = 1.0, stream: int = 0):
+        _check(self._lib.shafft_sm100_execute_step(self.handle, int(step), ctypes.c_void_p(src_ptr),
+                                                   ctypes.c_void_p(dst_ptr), int(direction),
+                                                   float(scale), ctypes.c_void_p(stream)),
+               "execute_step")
+
+    def step_bytes(self, step: int) -> int:
+        return int(self._lib.shafft_sm100_step_bytes(self.handle, int(step)))
 
     def describe(self) -> dict:
         buf = ctypes.create_string_buffer(1 << 16)

@@ -1,0 +1,44 @@
+// Host-side launchers of the device kernels, one explicit instantiation per
+// element type (launch_f32.cu, launch_f64.cu), so that the planner in
+// plan.cu stays plain host code and the kernel TUs compile in parallel.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pass.h"
+
+namespace shafft_sm100 {
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+
+template <typename T>
+struct Launch {
+  using C = typename Vec2<T>::type;
+  // raise the dynamic shared-memory limit of every pass kernel once
+  static cudaError_t init();
+  static cudaError_t pass(const PassGeom& g, const C* in, C* out, const PassTables<C>& tb,
+                          size_t smem, cudaStream_t s);
+  static cudaError_t scale_copy(const C* src, C* dst, int64_t n, T factor, int conj, cudaStream_t s);
+  static cudaError_t bs_modulate(const C* src, C* dst, int64_t L, int64_t M, int64_t I,
+                                 int64_t total, const C* chirp, int conj, cudaStream_t s);
+  static cudaError_t bs_mulh(C* s_, const C* H, int64_t M, int64_t total, cudaStream_t s);
+  static cudaError_t bs_demod(const C* src, C* dst, int64_t L, int64_t M, int64_t I, int64_t total,
+                              const C* chirp, int conj, T scale, cudaStream_t s);
+  static cudaError_t gen_twiddle(C* out, int64_t count, int64_t mult, int64_t N, cudaStream_t s);
+  static cudaError_t gen_chirp(C* out, int64_t L, cudaStream_t s);
+  static cudaError_t gen_bs_kernel(C* h, const C* chirp, int64_t L, int64_t M, cudaStream_t s);
+};
+
+extern template struct Launch<float>;
+extern template struct Launch<double>;
+
+}  // namespace shafft_sm100

@@ -1,0 +1,5 @@
+// double (complex128) instantiation of the kernel launchers.
+#include "launch_impl.cuh"
+namespace shafft_sm100 {
+template struct Launch<double>;
+}

@@ -36,7 +36,7 @@
 #include <vector>
 
 #include "../../../include/shafft_sm100.h"
-#include "kernels.cuh"
+#include "launch.h"
 #include "pass.h"
 
 namespace shafft_sm100 {
@@ -511,18 +511,16 @@ namespace {
 
 template <typename T>
 struct Launcher {
-  using C = typename Cx<T>::type;
+  using C = typename Vec2<T>::type;
+  using K = Launch<T>;
 
-  static int set_smem_attrs() {
+  static int init_once() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
-    std::call_once(once, [] {
-      err = cudaFuncSetAttribute(k_fft_pass<T, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 200 * 1024);
-    });
+    std::call_once(once, [] { err = K::init(); });
     if (err != cudaSuccess) {
       g_last_cuda = (int)err;
-      return set_err(SHAFFT_SM100_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(err));
+      return set_err(SHAFFT_SM100_ECUDA, "kernel attribute setup: %s", cudaGetErrorString(err));
     }
     return 0;
   }
@@ -541,9 +539,17 @@ struct Launcher {
     return tb;
   }
 
+  static int check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+      g_last_cuda = (int)e;
+      return set_err(SHAFFT_SM100_ECUDA, "%s launch: %s", what, cudaGetErrorString(e));
+    }
+    return 0;
+  }
+
   static int pass(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* out,
                   bool conj_in, bool conj_out, double scale, cudaStream_t s) {
-    int rc = set_smem_attrs();
+    int rc = init_once();
     if (rc) return rc;
     PassGeom g = st.g;
     g.conj_in = conj_in;
@@ -554,48 +560,36 @@ struct Launcher {
       g.tw_shift = nt.shift;
       g.tw_mask = nt.mask;
     }
-    PassTables<C> tb = tables(p, st);
-    int64_t grid = std::min<int64_t>(g.ntiles, 148 * 64);
-    k_fft_pass<T, 0, 0><<<(unsigned)grid, kThreads, st.smem, s>>>(
-        g, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), tb);
-    CUDA_TRY(cudaGetLastError());
-    return 0;
-  }
-
-  static unsigned grid_for(int64_t n) {
-    int64_t g = (n + 255) / 256;
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+    return check(K::pass(g, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), tables(p, st),
+                         st.smem, s),
+                 "fft pass");
   }
 
   static int elementwise(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* out,
                          bool conj_in, bool conj_out, double scale, cudaStream_t s) {
     const C* cin = reinterpret_cast<const C*>(in);
     C* cout = reinterpret_cast<C*>(out);
-    if (st.kind == ST_COPY) {
-      k_scale_copy<T><<<grid_for(st.total), 256, 0, s>>>(cin, cout, st.total, (T)scale,
-                                                        (conj_in != conj_out) ? 1 : 0);
-    } else {
-      const BTable& bt = p->btabs[st.tabB];
-      const C* chirp = reinterpret_cast<const C*>(p->d_tables + bt.off_chirp);
-      const C* H = reinterpret_cast<const C*>(p->d_tables + bt.off_H);
-      if (st.kind == ST_BS_MOD) {
-        k_bs_modulate<T><<<grid_for(st.total), 256, 0, s>>>(cin, cout, st.bsL, st.bsM, st.bsI,
-                                                           st.total, chirp, conj_in ? 1 : 0);
-      } else if (st.kind == ST_BS_MULH) {
-        k_bs_mulh<T><<<grid_for(st.total), 256, 0, s>>>(cout, H, st.bsM, st.total);
-      } else {
-        k_bs_demod<T><<<grid_for(st.total), 256, 0, s>>>(cin, cout, st.bsL, st.bsM, st.bsI, st.total,
-                                                        chirp, conj_out ? 1 : 0, (T)scale);
-      }
-    }
-    CUDA_TRY(cudaGetLastError());
-    return 0;
+    if (st.kind == ST_COPY)
+      return check(K::scale_copy(cin, cout, st.total, (T)scale, (conj_in != conj_out) ? 1 : 0, s),
+                   "copy");
+    const BTable& bt = p->btabs[st.tabB];
+    const C* chirp = reinterpret_cast<const C*>(p->d_tables + bt.off_chirp);
+    const C* H = reinterpret_cast<const C*>(p->d_tables + bt.off_H);
+    if (st.kind == ST_BS_MOD)
+      return check(K::bs_modulate(cin, cout, st.bsL, st.bsM, st.bsI, st.total, chirp,
+                                  conj_in ? 1 : 0, s),
+                   "bluestein modulate");
+    if (st.kind == ST_BS_MULH) return check(K::bs_mulh(cout, H, st.bsM, st.total, s), "bluestein multiply");
+    return check(K::bs_demod(cin, cout, st.bsL, st.bsM, st.bsI, st.total, chirp, conj_out ? 1 : 0,
+                             (T)scale, s),
+                 "bluestein demodulate");
   }
 
   static int run_steps(const shafft_sm100_plan_s* p, const std::vector<Step>& steps, void* const bufs[4],
-                       bool conj, double scale, cudaStream_t s) {
+                       bool conj, double scale, cudaStream_t s, int only = -1) {
     const size_t n = steps.size();
     for (size_t i = 0; i < n; ++i) {
+      if (only >= 0 && (size_t)only != i) continue;
       const Step& st = steps[i];
       const bool first = (i == 0), last = (i + 1 == n);
       const bool cin = first && conj;
@@ -614,9 +608,10 @@ struct Launcher {
   // Build every table of the plan on the device.
   static int build_tables(shafft_sm100_plan_s* p) {
     for (const LTable& lt : p->ltabs) {
-      k_gen_twiddle<T><<<grid_for(lt.L), 256, 0, p->stream>>>(
-          reinterpret_cast<C*>(p->d_tables + lt.off_tw), lt.L, 1, lt.L);
-      CUDA_TRY(cudaGetLastError());
+      int rc = check(K::gen_twiddle(reinterpret_cast<C*>(p->d_tables + lt.off_tw), lt.L, 1, lt.L,
+                                    p->stream),
+                     "twiddle generation");
+      if (rc) return rc;
       std::vector<uint16_t> p2k, k2p;
       digit_tables(lt.L, p2k, k2p);
       CUDA_TRY(cudaMemcpyAsync(p->d_tables + lt.off_p2k, p2k.data(), 2 * lt.L,
@@ -626,20 +621,24 @@ struct Launcher {
       CUDA_TRY(cudaStreamSynchronize(p->stream));
     }
     for (const NTable& nt : p->ntabs) {
-      k_gen_twiddle<T><<<grid_for(nt.nhi), 256, 0, p->stream>>>(
-          reinterpret_cast<C*>(p->d_tables + nt.off_hi), nt.nhi, nt.nlo, nt.N);
-      k_gen_twiddle<T><<<grid_for(nt.nlo), 256, 0, p->stream>>>(
-          reinterpret_cast<C*>(p->d_tables + nt.off_lo), nt.nlo, 1, nt.N);
-      CUDA_TRY(cudaGetLastError());
+      int rc = check(K::gen_twiddle(reinterpret_cast<C*>(p->d_tables + nt.off_hi), nt.nhi, nt.nlo,
+                                    nt.N, p->stream),
+                     "twiddle generation");
+      if (rc) return rc;
+      rc = check(K::gen_twiddle(reinterpret_cast<C*>(p->d_tables + nt.off_lo), nt.nlo, 1, nt.N,
+                                p->stream),
+                 "twiddle generation");
+      if (rc) return rc;
     }
     for (const BTable& bt : p->btabs) {
       C* chirp = reinterpret_cast<C*>(p->d_tables + bt.off_chirp);
-      k_gen_chirp<T><<<grid_for(bt.L), 256, 0, p->stream>>>(chirp, bt.L);
-      k_gen_bs_kernel<T><<<grid_for(bt.M), 256, 0, p->stream>>>(reinterpret_cast<C*>(p->d_s0),
-                                                               chirp, bt.L, bt.M);
-      CUDA_TRY(cudaGetLastError());
+      int rc = check(K::gen_chirp(chirp, bt.L, p->stream), "chirp generation");
+      if (rc) return rc;
+      rc = check(K::gen_bs_kernel(reinterpret_cast<C*>(p->d_s0), chirp, bt.L, bt.M, p->stream),
+                 "bluestein kernel generation");
+      if (rc) return rc;
       void* bufs[4] = {nullptr, nullptr, p->d_s0, p->d_s1};
-      int rc = run_steps(p, bt.hsteps, bufs, false, 1.0 / (double)bt.M, p->stream);
+      rc = run_steps(p, bt.hsteps, bufs, false, 1.0 / (double)bt.M, p->stream);
       if (rc) return rc;
       CUDA_TRY(cudaMemcpyAsync(p->d_tables + bt.off_H, bufs[bt.hresult_buf], sizeof(C) * bt.M,
                                cudaMemcpyDeviceToDevice, p->stream));
@@ -802,21 +801,46 @@ int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direc
              : Launcher<float>::run_steps(plan, plan->steps, bufs, direction == 1, scale, s);
 }
 
+int shafft_sm100_execute_step(shafft_sm100_plan plan, int step, void* src, void* dst, int direction,
+                              double scale, void* stream) {
+  if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
+  if (step < 0 || step >= (int)plan->steps.size()) return set_err(SHAFFT_SM100_EINVAL, "bad step");
+  if (!src || !dst || src == dst) return set_err(SHAFFT_SM100_EINVAL, "bad buffers");
+  cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : plan->stream;
+  void* bufs[4] = {src, dst, plan->d_s0, plan->d_s1};
+  return plan->precision
+             ? Launcher<double>::run_steps(plan, plan->steps, bufs, direction == 1, scale, s, step)
+             : Launcher<float>::run_steps(plan, plan->steps, bufs, direction == 1, scale, s, step);
+}
+
+int64_t shafft_sm100_step_bytes(shafft_sm100_plan plan, int step) {
+  if (!plan || step < 0 || step >= (int)plan->steps.size()) return 0;
+  const Step& st = plan->steps[step];
+  const int64_t es = plan->precision ? 16 : 8;
+  if (st.kind == ST_PASS) {
+    int64_t n = (int64_t)st.g.L;
+    for (int d = 0; d < 4; ++d) n *= st.g.ext[d];
+    return 2 * n * es;
+  }
+  if (st.kind == ST_BS_MOD) return (st.total / st.bsM * st.bsL + st.total) * es;
+  if (st.kind == ST_BS_DEMOD) return (st.total / st.bsL * st.bsL + st.total) * es;
+  return 2 * st.total * es;
+}
+
 int shafft_sm100_scale(void* data, size_t count, int precision, double factor, void* stream) {
   if (!data && count) return set_err(SHAFFT_SM100_EINVAL, "null buffer");
   if (precision != 0 && precision != 1) return set_err(SHAFFT_SM100_EINVAL, "bad precision");
   if (count == 0) return 0;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int64_t n = (int64_t)count;
-  unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32));
-  if (precision) {
-    k_scale_copy<double><<<grid, 256, 0, s>>>(reinterpret_cast<const double2*>(data),
-                                               reinterpret_cast<double2*>(data), n, factor, 0);
-  } else {
-    k_scale_copy<float><<<grid, 256, 0, s>>>(reinterpret_cast<const float2*>(data),
-                                              reinterpret_cast<float2*>(data), n, (float)factor, 0);
-  }
-  CUDA_TRY(cudaGetLastError());
+  cudaError_t e;
+  if (precision)
+    e = Launch<double>::scale_copy(reinterpret_cast<const double2*>(data),
+                                   reinterpret_cast<double2*>(data), n, factor, 0, s);
+  else
+    e = Launch<float>::scale_copy(reinterpret_cast<const float2*>(data),
+                                  reinterpret_cast<float2*>(data), n, (float)factor, 0, s);
+  CUDA_TRY(e);
   return 0;
 }
 
@@ -839,6 +863,56 @@ size_t shafft_sm100_plan_device_bytes(shafft_sm100_plan plan) {
 int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen) {
   if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
   return copy_out(describe_steps(plan->precision, plan->steps, plan->total), buf, buflen);
+}
+
+int shafft_sm100_malloc(void** ptr, size_t bytes) {
+  if (!ptr) return set_err(SHAFFT_SM100_EINVAL, "null pointer");
+  *ptr = nullptr;
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    g_last_cuda = (int)e;
+    *ptr = nullptr;
+    return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  return 0;
+}
+
+int shafft_sm100_free(void* ptr) {
+  if (!ptr) return 0;
+  CUDA_TRY(cudaFree(ptr));
+  return 0;
+}
+
+int shafft_sm100_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
+  if (!bytes) return 0;
+  if (!dst || !src) return set_err(SHAFFT_SM100_EINVAL, "null pointer");
+  cudaMemcpyKind k = kind == SHAFFT_SM100_H2D   ? cudaMemcpyHostToDevice
+                     : kind == SHAFFT_SM100_D2H ? cudaMemcpyDeviceToHost
+                     : kind == SHAFFT_SM100_D2D ? cudaMemcpyDeviceToDevice
+                                                : cudaMemcpyDefault;
+  if (stream) {
+    CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, k, reinterpret_cast<cudaStream_t>(stream)));
+  } else {
+    CUDA_TRY(cudaMemcpy(dst, src, bytes, k));
+  }
+  return 0;
+}
+
+int shafft_sm100_stream_sync(void* stream) {
+  CUDA_TRY(cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)));
+  return 0;
+}
+
+int shafft_sm100_device_name(char* buf, int buflen) {
+  if (!buf || buflen <= 0) return set_err(SHAFFT_SM100_EINVAL, "bad buffer");
+  buf[0] = 0;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, dev));
+  snprintf(buf, buflen, "%s", prop.name);
+  return 0;
 }
 
 int shafft_sm100_last_cuda_error(void) { return g_last_cuda; }

@@ -1,0 +1,166 @@
+"""C-ABI boundary checks that need no GPU: the libraries load, export every
+function include/*.h declares, and the host state machine returns the
+reference's status codes (src/cpp/shafft.cpp, src/cpp/shafft_internal.cpp)."""
+import ctypes
+import os
+import re
+import threading
+
+import pytest
+
+import shafft_b200 as S
+from shafft_b200 import _sm100
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions(header):
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    names = set()
+    for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(([^;{)]*)\)\s*;", text):
+        name = m.group(1)
+        if name in ("if", "while", "sizeof", "return", "switch", "defined"):
+            continue
+        pre = text[max(0, m.start() - 80):m.start()]
+        if "typedef" in pre.split(";")[-1] or "#define" in pre.split("\n")[-1]:
+            continue
+        names.add(name)
+    return names
+
+
+@pytest.mark.parametrize("header,lib", [
+    ("include/shafft/shafft.h", "shafft_b200/lib/libshafft.so"),
+    ("include/shafft_sm100.h", "shafft_b200/lib/libshafft_sm100.so"),
+    ("include/mpi_shim/mpi.h", "shafft_b200/lib/libshafft_mpishim.so"),
+])
+def test_every_declared_symbol_is_exported(header, lib):
+    names = declared_functions(os.path.join(ROOT, header))
+    assert len(names) > 5
+    so = ctypes.CDLL(os.path.join(ROOT, lib))
+    missing = [n for n in sorted(names) if not hasattr(so, n)]
+    assert not missing, missing
+
+
+def test_backend_and_version():
+    assert S.backend_name() == "sm100"
+    assert S.version_string() == "1.1.0-alpha"
+    a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    S.load().shafftGetVersion(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    assert (a.value, b.value, c.value) == (1, 1, 0)
+
+
+def test_nd_state_machine_without_gpu():
+    p = S.FFTND()
+    assert not p.is_configured()
+    assert p.plan() == S.ERR_PLAN_NOT_INIT                      # plan before init
+    assert p.execute(S.FORWARD) == S.ERR_PLAN_NOT_INIT          # execute before plan
+    assert p.normalize() == S.ERR_PLAN_NOT_INIT                 # normalize before plan
+    assert p.init([1, 1, 1], [64, 64, 32]) == 0
+    assert p.is_configured() and p.is_active()
+    assert p.alloc_size() == 64 * 64 * 32 and p.global_size() == 64 * 64 * 32
+    assert p.init([1, 1, 1], [64, 64, 32]) == S.ERR_INVALID_STATE  # re-init
+    assert p.set_buffers(0, 0) == S.ERR_NULLPTR
+    rc, d, w = p.get_buffers()
+    assert rc == S.ERR_NO_BUFFER and d == 0 and w == 0
+    assert p.execute(S.FORWARD) == S.ERR_PLAN_NOT_INIT
+    rc, sub, off = p.get_layout()
+    assert rc == 0 and sub == [64, 64, 32] and off == [0, 0, 0]
+    rc, ca, da = p.get_axes()
+    assert rc == 0 and ca == [0, 1, 2]
+
+
+@pytest.mark.parametrize("comm_dims,dims,code", [
+    ([1, 1, 2], [4, 4, 4], S.ERR_INVALID_DECOMP),   # last axis distributed
+    ([0, 1, 1], [4, 4, 4], S.ERR_INVALID_DECOMP),   # unresolved zeros (resolve through configurationND)
+    ([2, 1, 1], [4, 4, 4], S.ERR_INVALID_DECOMP),   # grid of 2 on one rank
+    ([1, 1, 1], [4, 0, 4], S.ERR_INVALID_DIM),
+])
+def test_nd_init_errors(comm_dims, dims, code):
+    p = S.FFTND()
+    assert p.init(comm_dims, dims) == code
+    assert S.load().shafftLastErrorStatus() == code
+
+
+def test_nd_init_bad_type_and_null():
+    p = S.FFTND()
+    assert p.init([1], [8], precision=7) == S.ERR_INVALID_FFTTYPE
+    lib = S.load()
+    assert lib.shafftNDInit(None, 1, None, None, 0, S.MPI_COMM_WORLD, 0) == S.ERR_NULLPTR
+    assert lib.shafftPlan(None) == S.ERR_NULLPTR
+    assert lib.shafftExecute(None, 0) == S.ERR_NULLPTR
+
+
+def test_inactive_rank_plan_is_noop():
+    # plan_data_base.hpp:35-58 -- inactive ranks (MPI_COMM_NULL) execute nothing
+    p = S.FFTND()
+    assert p.init([1, 1], [8, 8], comm=S.MPI_COMM_NULL) == 0
+    assert not p.is_active() and p.alloc_size() == 0
+    assert p.plan() == 0
+    assert p.set_buffers(0, 0) == 0
+    assert p.execute(S.FORWARD) == 0 and p.normalize() == 0
+
+
+def test_fft1d_configuration_and_errors():
+    rc, ln, ls, al = S.configuration_1d(1000003)
+    assert (rc, ln, ls, al) == (0, 1000003, 0, 1000003)
+    p = S.FFT1D()
+    assert p.plan() == S.ERR_PLAN_NOT_INIT    # shafftPlan -> fft1dCreatePlans before init (shafft_internal.cpp:760-770)
+    assert p.init(1 << 31) == S.ERR_SIZE_OVERFLOW
+    q = S.FFT1D()
+    assert q.init(0) == S.ERR_INVALID_DIM
+    r = S.FFT1D()
+    assert r.init(4096) == 0 and r.alloc_size() == 4096
+    assert r.init(4096) == S.ERR_INVALID_STATE
+
+
+def test_configuration_nd():
+    rc, cd, nda, sub, off, cs = S.configuration_nd([64, 64, 32])
+    assert rc == 0 and cd == [1, 1, 1] and nda == 0 and sub == [64, 64, 32] and off == [0, 0, 0] and cs == 1
+    # memLimit counts data + work buffers (configuration.cpp:26-58)
+    rc, *_ = S.configuration_nd([64, 64, 32], mem_limit=2 * 8 * 64 * 64 * 32)
+    assert rc == 0
+    rc, *_ = S.configuration_nd([64, 64, 32], mem_limit=2 * 8 * 64 * 64 * 32 - 1)
+    assert rc == S.ERR_INVALID_DECOMP
+
+
+def test_error_state_is_thread_local():
+    lib = S.load()
+    p = S.FFTND()
+    assert p.init([1, 1, 2], [4, 4, 4]) == S.ERR_INVALID_DECOMP
+    seen = {}
+
+    def other():
+        lib.shafftClearLastError()
+        seen["status"] = lib.shafftLastErrorStatus()
+    t = threading.Thread(target=other)
+    t.start()
+    t.join()
+    assert seen["status"] == 0
+    assert lib.shafftLastErrorStatus() == S.ERR_INVALID_DECOMP
+    assert lib.shafftErrorSourceName(0) == b"SHAFFT"
+    assert lib.shafftErrorSourceName(2) == b"CUDA"
+    lib.shafftClearLastError()
+    assert lib.shafftLastErrorStatus() == 0
+
+
+def test_planner_pass_lists():
+    """Host-only planner: pass structure of the headline and config shapes."""
+    q = _sm100.plan_query([512, 512, 512], 0)
+    assert [s["kind"] for s in q["steps"]] == ["pass"] * len(q["steps"])
+    assert len(q["steps"]) <= 3
+    q = _sm100.plan_query([256, 256, 256], 1)
+    assert len(q["steps"]) <= 3
+    q = _sm100.plan_query([1000003], 0)
+    kinds = [s["kind"] for s in q["steps"]]
+    assert kinds[0] == "bluestein_modulate" and kinds[-1] == "bluestein_demodulate"
+    assert q["steps"][0]["M"] == 1 << 21
+    q = _sm100.plan_query([1488375], 0)
+    assert all(s["kind"] == "pass" for s in q["steps"]) and len(q["steps"]) == 2
+    q = _sm100.plan_query([1, 1, 1], 0)
+    assert [s["kind"] for s in q["steps"]] == ["copy"]
+    # the final step always writes the destination buffer
+    for dims in ([63, 47, 31], [1 << 24], [4096, 3], [7, 11, 13, 17], [2, 3, 4, 5]):
+        q = _sm100.plan_query(dims, 0)
+        assert q["steps"][-1]["out"] == "dst", dims
