@@ -1,0 +1,258 @@
+// Specialised HBM pass for hot lengths (compile-time L and radix plan).
+//
+// One CTA transforms a tile of L points x W batch columns, W = 8 * VW where a
+// 16-byte "chunk" holds VW complex elements (VW = 2 for complex64, 1 for
+// complex128), so a tile row is exactly one 128-byte line.
+//
+// Phase A  every thread issues all the loads of its first-stage butterflies
+//          before any arithmetic (R0 * NB0 * VW independent loads in flight
+//          per thread), runs the radix-R0 butterflies in registers, applies
+//          the DIF twiddle and stores 16-byte chunks to shared memory.
+//          IN_ROW = false: the batch column is contiguous in HBM (column
+//          tile) -- 8 lanes read one 128-byte line per instruction.
+//          IN_ROW = true : the transform axis is contiguous (row tile) -- 32
+//          lanes read 32 consecutive points of one row per instruction.
+// Phase B  middle radix stages in shared memory.
+// Phase C  last radix stage; the result is written straight from registers
+//          to HBM in natural (digit-unreversed) order, 8 lanes per 128-byte
+//          line, with scale / conjugation / four-step post-twiddle fused.
+//          The output is always a column tile, so with IN_ROW the pass also
+//          transposes (rotate-on-write).
+// Shared layout: row p holds 8 chunks; chunk c of row p is stored at slot
+// c ^ (p & 7).  Any 8 lanes that touch 8 different chunks of one row, or the
+// same chunk of 8 rows with distinct p mod 8, hit 8 different 16-byte bank
+// groups, so every phase is free of bank conflicts.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "butterflies.cuh"
+#include "pass.h"
+
+namespace shafft_sm100 {
+
+template <typename T>
+struct ChunkT;
+template <>
+struct ChunkT<float> {
+  static constexpr int VW = 2;
+};
+template <>
+struct ChunkT<double> {
+  static constexpr int VW = 1;
+};
+
+template <int L, int R0, int R1, int R2, int NT>
+struct FastCfg {
+  static constexpr int S = (R2 > 1) ? 3 : 2;
+  static_assert(R0 * R1 * (R2 > 1 ? R2 : 1) == L, "radices must multiply to L");
+  static constexpr int NB0 = L * 8 / (R0 * NT);
+  static constexpr int NB1 = L * 8 / (R1 * NT);
+  static constexpr int NB2 = (R2 > 1) ? L * 8 / (R2 * NT) : 1;
+  static_assert(NB0 >= 1 && NB0 * R0 * NT == L * 8, "stage 0 must tile the threads");
+  static_assert(NB1 >= 1 && NB1 * R1 * NT == L * 8, "stage 1 must tile the threads");
+  static_assert(R2 <= 1 || (NB2 >= 1 && NB2 * R2 * NT == L * 8), "stage 2 must tile the threads");
+};
+
+// 16-byte chunk I/O
+template <typename C, int VW>
+struct Chunk {
+  C v[VW];
+};
+
+__device__ __forceinline__ int swz(int p, int c) { return p * 8 + (c ^ (p & 7)); }
+
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW>
+__global__ void __launch_bounds__(NT)
+    k_fft_fast(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
+               typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+  using C = typename Cx<T>::type;
+  using Cfg = FastCfg<L, R0, R1, R2, NT>;
+  constexpr int VW = ChunkT<T>::VW;
+  constexpr int W = 8 * VW;
+  constexpr int S = Cfg::S;
+  constexpr int RL = (S == 3) ? R2 : R1;  // radix of the last stage
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sm = reinterpret_cast<float4*>(smem_raw);  // L rows x 8 chunks of 16 bytes
+
+  const int tid = threadIdx.x;
+  int64_t tile = blockIdx.x;
+  const int64_t tw = tile % g.tiles_w;
+  int64_t rest = tile / g.tiles_w;
+  const int64_t i1 = rest % g.ext[1];
+  rest /= g.ext[1];
+  const int64_t i2 = rest % g.ext[2];
+  const int64_t i3 = rest / g.ext[2];
+  const int64_t w0 = tw * W;
+  const int64_t bin = w0 * g.sin[0] + i1 * g.sin[1] + i2 * g.sin[2] + i3 * g.sin[3];
+  const int64_t bout = w0 + i1 * g.sout[1] + i2 * g.sout[2] + i3 * g.sout[3];
+  const int64_t tconst = g.tw_dim == 1 ? i1 : (g.tw_dim == 2 ? i2 : (g.tw_dim == 3 ? i3 : 0));
+
+  // ---------------- phase A: loads + radix-R0 stage ----------------
+  {
+    constexpr int M0 = L / R0;  // stride between the inputs of one butterfly
+    C v[Cfg::NB0][R0][VW];
+    int bj[Cfg::NB0], bc[Cfg::NB0];
+#pragma unroll
+    for (int b = 0; b < Cfg::NB0; ++b) {
+      const int id = tid + b * NT;  // chunk-butterfly id in [0, M0*8)
+      int j, c;
+      if (IN_ROW) {
+        j = id % M0;
+        c = id / M0;
+      } else {
+        c = id & 7;
+        j = id >> 3;
+      }
+      bj[b] = j;
+      bc[b] = c;
+    }
+    // issue every load first
+#pragma unroll
+    for (int b = 0; b < Cfg::NB0; ++b) {
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int n = bj[b] + r * M0;
+        if (IN_ROW) {
+#pragma unroll
+          for (int e = 0; e < VW; ++e)
+            v[b][r][e] = in[bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n];
+        } else {
+          const Chunk<C, VW> ch =
+              *reinterpret_cast<const Chunk<C, VW>*>(in + bin + bc[b] * VW + (int64_t)n * g.sn_in);
+#pragma unroll
+          for (int e = 0; e < VW; ++e) v[b][r][e] = ch.v[e];
+        }
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < Cfg::NB0; ++b) {
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+        C x[R0];
+#pragma unroll
+        for (int r = 0; r < R0; ++r) {
+          x[r] = v[b][r][e];
+          if (g.conj_in) x[r].y = -x[r].y;
+        }
+        dft<R0>(x);
+        if (bj[b] != 0) {
+#pragma unroll
+          for (int r = 1; r < R0; ++r) x[r] = cmul(x[r], tb.twL[bj[b] * r]);
+        }
+#pragma unroll
+        for (int r = 0; r < R0; ++r) v[b][r][e] = x[r];
+      }
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        Chunk<C, VW> ch;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) ch.v[e] = v[b][r][e];
+        const int p = bj[b] + r * M0;
+        sm[swz(p, bc[b])] = *reinterpret_cast<float4*>(&ch);
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---------------- phase B: middle stage (3-stage plans) ----------------
+  if constexpr (S == 3) {
+    constexpr int SPAN = L / R0;
+    constexpr int M1 = SPAN / R1;
+#pragma unroll
+    for (int b = 0; b < Cfg::NB1; ++b) {
+      const int id = tid + b * NT;
+      const int c = id & 7;
+      const int q = id >> 3;  // [0, L/R1)
+      const int blk = q / M1, j = q % M1;
+      const int base = blk * SPAN + j;
+      C x[R1][VW];
+#pragma unroll
+      for (int r = 0; r < R1; ++r) {
+        float4 raw = sm[swz(base + r * M1, c)];
+        const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) x[r][e] = ch.v[e];
+      }
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+        C y[R1];
+#pragma unroll
+        for (int r = 0; r < R1; ++r) y[r] = x[r][e];
+        dft<R1>(y);
+        if (j != 0) {
+#pragma unroll
+          for (int r = 1; r < R1; ++r) y[r] = cmul(y[r], tb.twL[j * r * R0]);
+        }
+#pragma unroll
+        for (int r = 0; r < R1; ++r) x[r][e] = y[r];
+      }
+#pragma unroll
+      for (int r = 0; r < R1; ++r) {
+        Chunk<C, VW> ch;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) ch.v[e] = x[r][e];
+        sm[swz(base + r * M1, c)] = *reinterpret_cast<float4*>(&ch);
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---------------- phase C: last stage, natural-order store ----------------
+  {
+    constexpr int NBL = (S == 3) ? Cfg::NB2 : Cfg::NB1;
+    const T scale = (T)g.scale;
+#pragma unroll
+    for (int b = 0; b < NBL; ++b) {
+      const int id = tid + b * NT;
+      const int c = id & 7;
+      const int blk = id >> 3;  // [0, L/RL)
+      // digits of blk: 3 stages: blk = d0*R1 + d1 ; 2 stages: blk = d0
+      int kbase;
+      if constexpr (S == 3) {
+        const int d0 = blk / R1, d1 = blk % R1;
+        kbase = d0 + R0 * d1;
+      } else {
+        kbase = blk;
+      }
+      constexpr int KSTRIDE = L / RL;  // output stride of the last digit
+      C x[RL][VW];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        float4 raw = sm[swz(blk * RL + r, c)];
+        const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) x[r][e] = ch.v[e];
+      }
+#pragma unroll
+      for (int e = 0; e < VW; ++e) {
+        C y[RL];
+#pragma unroll
+        for (int r = 0; r < RL; ++r) y[r] = x[r][e];
+        dft<RL>(y);
+#pragma unroll
+        for (int r = 0; r < RL; ++r) x[r][e] = y[r];
+      }
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int k = kbase + r * KSTRIDE;
+        Chunk<C, VW> ch;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+          C y = x[r][e];
+          if (g.tw_mode == TW_POST) {
+            const int64_t t = (g.tw_dim == 0) ? (w0 + c * VW + e) : tconst;
+            const int64_t m = (int64_t)k * t;
+            y = cmul(y, cmul(tb.tw_hi[m >> g.tw_shift], tb.tw_lo[m & g.tw_mask]));
+          }
+          if (g.scale != 1.0) y = cscale(y, scale);
+          if (g.conj_out) y.y = -y.y;
+          ch.v[e] = y;
+        }
+        *reinterpret_cast<Chunk<C, VW>*>(out + bout + c * VW + (int64_t)k * g.sk_out) = ch;
+      }
+    }
+  }
+}
+
+}  // namespace shafft_sm100

@@ -27,6 +27,13 @@ struct Launch {
   static cudaError_t init();
   static cudaError_t pass(const PassGeom& g, const C* in, C* out, const PassTables<C>& tb,
                           size_t smem, cudaStream_t s);
+  // specialised pass for a hot length; tile width is 16 bytes x 8 (= 8*VW
+  // elements), output is a column tile.  Returns cudaErrorNotSupported when
+  // no specialisation exists for L.
+  static cudaError_t fast(const PassGeom& g, bool in_row, const C* in, C* out,
+                          const PassTables<C>& tb, cudaStream_t s);
+  static bool fast_supported(int L);
+  static int fast_threads(int L);
   static cudaError_t scale_copy(const C* src, C* dst, int64_t n, T factor, int conj, cudaStream_t s);
   static cudaError_t bs_modulate(const C* src, C* dst, int64_t L, int64_t M, int64_t I,
                                  int64_t total, const C* chirp, int conj, cudaStream_t s);
@@ -37,6 +44,22 @@ struct Launch {
   static cudaError_t gen_chirp(C* out, int64_t L, cudaStream_t s);
   static cudaError_t gen_bs_kernel(C* h, const C* chirp, int64_t L, int64_t M, cudaStream_t s);
 };
+
+// per-precision specialisations (defined in launch_f32.cu / launch_f64.cu)
+template <>
+bool Launch<float>::fast_supported(int L);
+template <>
+bool Launch<double>::fast_supported(int L);
+template <>
+int Launch<float>::fast_threads(int L);
+template <>
+int Launch<double>::fast_threads(int L);
+template <>
+cudaError_t Launch<float>::fast(const PassGeom& g, bool in_row, const float2* in, float2* out,
+                                const PassTables<float2>& tb, cudaStream_t s);
+template <>
+cudaError_t Launch<double>::fast(const PassGeom& g, bool in_row, const double2* in, double2* out,
+                                 const PassTables<double2>& tb, cudaStream_t s);
 
 extern template struct Launch<float>;
 extern template struct Launch<double>;

@@ -1,4 +1,5 @@
 // float (complex64) instantiation of the kernel launchers.
+#define SHAFFT_INSTANTIATE_F32 1
 #include "launch_impl.cuh"
 namespace shafft_sm100 {
 template struct Launch<float>;

@@ -3,6 +3,7 @@
 #pragma once
 #include <algorithm>
 
+#include "fast.cuh"
 #include "kernels.cuh"
 #include "launch.h"
 
@@ -13,11 +14,147 @@ static inline unsigned ew_grid(int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
 }
 
+// Compile-time radix plans of the specialised passes: (L, R0, R1, R2, threads).
+// Every stage gives each thread a whole number of 16-byte-chunk butterflies.
+template <typename T>
+struct FastTable;
+#define SHAFFT_FAST_LIST_F32(X) \
+  X(16, 4, 4, 1, 32)            \
+  X(32, 8, 4, 1, 32)            \
+  X(64, 8, 8, 1, 64)            \
+  X(128, 8, 4, 4, 128)          \
+  X(256, 8, 8, 4, 256)          \
+  X(512, 8, 8, 8, 256)          \
+  X(1024, 8, 8, 16, 512)
+#define SHAFFT_FAST_LIST_F64(X) \
+  X(16, 4, 4, 1, 32)            \
+  X(32, 8, 4, 1, 32)            \
+  X(64, 8, 8, 1, 64)            \
+  X(128, 8, 4, 4, 128)          \
+  X(256, 8, 8, 4, 128)          \
+  X(512, 8, 8, 8, 256)
+
+template <typename T>
+static cudaError_t fast_attr_all();
+
+#ifdef SHAFFT_INSTANTIATE_F32
+template <>
+cudaError_t fast_attr_all<float>() {
+  cudaError_t e = cudaSuccess;
+#define SHAFFT_ATTR(L, A, B, C_, NT)                                                             \
+  if (e == cudaSuccess)                                                                          \
+    e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, false>,                          \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);              \
+  if (e == cudaSuccess)                                                                          \
+    e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, true>,                           \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+  SHAFFT_FAST_LIST_F32(SHAFFT_ATTR)
+#undef SHAFFT_ATTR
+  return e;
+}
+#endif
+#ifdef SHAFFT_INSTANTIATE_F64
+template <>
+cudaError_t fast_attr_all<double>() {
+  cudaError_t e = cudaSuccess;
+#define SHAFFT_ATTR(L, A, B, C_, NT)                                                             \
+  if (e == cudaSuccess)                                                                          \
+    e = cudaFuncSetAttribute(k_fft_fast<double, L, A, B, C_, NT, false>,                         \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);              \
+  if (e == cudaSuccess)                                                                          \
+    e = cudaFuncSetAttribute(k_fft_fast<double, L, A, B, C_, NT, true>,                          \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+  SHAFFT_FAST_LIST_F64(SHAFFT_ATTR)
+#undef SHAFFT_ATTR
+  return e;
+}
+
+#endif
+
 template <typename T>
 cudaError_t Launch<T>::init() {
-  return cudaFuncSetAttribute(k_fft_pass<T, 0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              200 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(k_fft_pass<T, 0, 0>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  return fast_attr_all<T>();
 }
+
+
+
+#ifdef SHAFFT_INSTANTIATE_F32
+template <>
+bool Launch<float>::fast_supported(int L) {
+  switch (L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
+    SHAFFT_FAST_LIST_F32(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return false;
+  }
+}
+template <>
+int Launch<float>::fast_threads(int L) {
+  switch (L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return NT;
+    SHAFFT_FAST_LIST_F32(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return 0;
+  }
+}
+template <>
+cudaError_t Launch<float>::fast(const PassGeom& g, bool in_row, const C* in, C* out,
+                                const PassTables<C>& tb, cudaStream_t s) {
+  const unsigned grid = (unsigned)g.ntiles;
+  switch (g.L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT)                                                          \
+  case L_:                                                                                     \
+    if (in_row)                                                                                \
+      k_fft_fast<float, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);    \
+    else                                                                                       \
+      k_fft_fast<float, L_, A, B, C_, NT, false><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);   \
+    return cudaGetLastError();
+    SHAFFT_FAST_LIST_F32(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return cudaErrorNotSupported;
+  }
+}
+#endif
+#ifdef SHAFFT_INSTANTIATE_F64
+template <>
+bool Launch<double>::fast_supported(int L) {
+  switch (L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
+    SHAFFT_FAST_LIST_F64(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return false;
+  }
+}
+template <>
+int Launch<double>::fast_threads(int L) {
+  switch (L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return NT;
+    SHAFFT_FAST_LIST_F64(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return 0;
+  }
+}
+template <>
+cudaError_t Launch<double>::fast(const PassGeom& g, bool in_row, const C* in, C* out,
+                                 const PassTables<C>& tb, cudaStream_t s) {
+  const unsigned grid = (unsigned)g.ntiles;
+  switch (g.L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT)                                                          \
+  case L_:                                                                                     \
+    if (in_row)                                                                                \
+      k_fft_fast<double, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);   \
+    else                                                                                       \
+      k_fft_fast<double, L_, A, B, C_, NT, false><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);  \
+    return cudaGetLastError();
+    SHAFFT_FAST_LIST_F64(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return cudaErrorNotSupported;
+  }
+}
+#endif
 
 template <typename T>
 cudaError_t Launch<T>::pass(const PassGeom& g, const C* in, C* out, const PassTables<C>& tb,

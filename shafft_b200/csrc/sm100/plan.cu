@@ -87,6 +87,8 @@ struct Step {
   int tabL = -1, tabN = -1, tabB = -1;
   int64_t bsL = 0, bsM = 0, bsI = 1, total = 0;
   size_t smem = 0;
+  int fast = 0;      // 1: specialised k_fft_fast pass (compile-time L)
+  int fast_row = 0;  // specialised pass reads row tiles (transposing)
 };
 
 struct LTable {
@@ -147,6 +149,38 @@ struct Planner {
   int64_t scratch_elems = 0;
 
   explicit Planner(int prec) : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {}
+
+  // specialised-pass eligibility: length, tile width and 16-byte alignment
+  int fast_w() const { return precision ? 8 : 16; }
+  int vw() const { return precision ? 1 : 2; }
+  bool fast_len(int64_t L) const {
+    if (L > 1 << 20) return false;
+    return precision ? Launch<double>::fast_supported((int)L) : Launch<float>::fast_supported((int)L);
+  }
+  bool fast_geom(const PassGeom& g, bool in_row) const {
+    const int v = vw();
+    if (g.ext[0] % fast_w() != 0) return false;
+    if (g.sout[0] != 1) return false;
+    if (!in_row && g.sin[0] != 1) return false;
+    if (in_row && g.sn_in != 1) return false;
+    if (g.sk_out % v) return false;
+    if (!in_row && g.sn_in % v) return false;
+    for (int d = 1; d < 4; ++d)
+      if (g.sout[d] % v || (!in_row && g.sin[d] % v)) return false;
+    return true;
+  }
+  // turn a planned generic pass into a specialised one when it qualifies
+  void try_fast(Step& st) {
+    PassGeom& g = st.g;
+    if (!fast_len(g.L) || g.tw_mode == TW_PRE) return;
+    const bool in_row = (g.sn_in == 1);
+    if (!fast_geom(g, in_row)) return;
+    if (in_row && st.in_buf == st.out_buf) return;  // transposing pass must be out of place
+    st.fast = 1;
+    st.fast_row = in_row ? 1 : 0;
+    finish_geom(st, fast_w());
+    st.smem = (size_t)g.L * 128;
+  }
 
   size_t alloc(size_t bytes) {
     size_t off = (table_bytes + 255) & ~size_t(255);
@@ -241,12 +275,60 @@ struct Planner {
       g.ext[2] = g.ext[3] = 1;
       g.sn_in = g.sk_out = I;
       finish_geom(st, W);
+      try_fast(st);
     }
     out.push_back(st);
   }
 
+  // The last two axes (A = rows, Lr = contiguous) as two transposing passes:
+  // rows of Lr -> [o][kL][a] in `mid`, then rows of A -> [o][ka][kL] in
+  // out_buf.  Both passes read row tiles and store column tiles.
+  bool transposed_pair(std::vector<Step>& out, int64_t O, int64_t A, int64_t Lr, int in_buf,
+                       int mid_buf, int out_buf) {
+    if (!fast_len(A) || !fast_len(Lr) || A % fast_w() || Lr % fast_w()) return false;
+    Step s1;
+    s1.kind = ST_PASS;
+    s1.in_buf = in_buf;
+    s1.out_buf = mid_buf;
+    fill_radix(s1.g, (int)Lr);
+    s1.g.ext[0] = A;  s1.g.sin[0] = Lr;  s1.g.sout[0] = 1;
+    s1.g.ext[1] = O;  s1.g.sin[1] = s1.g.sout[1] = A * Lr;
+    s1.g.ext[2] = s1.g.ext[3] = 1;
+    s1.g.sn_in = 1;
+    s1.g.sk_out = A;
+    finish_geom(s1, fast_w());
+    Step s2;
+    s2.kind = ST_PASS;
+    s2.in_buf = mid_buf;
+    s2.out_buf = out_buf;
+    fill_radix(s2.g, (int)A);
+    s2.g.ext[0] = Lr;  s2.g.sin[0] = A;  s2.g.sout[0] = 1;
+    s2.g.ext[1] = O;  s2.g.sin[1] = s2.g.sout[1] = A * Lr;
+    s2.g.ext[2] = s2.g.ext[3] = 1;
+    s2.g.sn_in = 1;
+    s2.g.sk_out = Lr;
+    finish_geom(s2, fast_w());
+    try_fast(s1);
+    try_fast(s2);
+    if (!s1.fast || !s2.fast) return false;
+    out.push_back(s1);
+    out.push_back(s2);
+    return true;
+  }
+
   // choose 2- or 3-factor split of a smooth L; returns empty if impossible
   std::vector<int> split(int64_t L, int64_t I) const {
+    // prefer factors that all have a specialised pass (largest last factor)
+    {
+      const int64_t fl[] = {1024, 512, 256, 128, 64};
+      for (int64_t d : fl) {
+        if (L % d || !fast_len(d)) continue;
+        const int64_t c = L / d;
+        if (fast_len(c)) return {(int)c, (int)d};
+        for (int64_t f : fl)
+          if (c % f == 0 && fast_len(f) && fast_len(c / f)) return {(int)(c / f), (int)f, (int)d};
+      }
+    }
     const int max_last = (I == 1) ? lim.max_row : lim.max_col;
     std::vector<int> best;
     // 2 factors: largest last factor whose cofactor fits a column pass
@@ -306,6 +388,7 @@ struct Planner {
       g.tw_mode = TW_POST;
       st.tabN = ntab(span);
       finish_geom(st, W);
+      try_fast(st);
       out.push_back(st);
       span = m;
     }
@@ -346,6 +429,7 @@ struct Planner {
         W = std::min(W, lim.w_col);
       }
       finish_geom(st, W);
+      try_fast(st);
       out.push_back(st);
     }
   }
@@ -434,34 +518,75 @@ struct Planner {
   }
 
   int plan_nd(std::vector<Step>& out, int ndim, const int64_t* dims) {
-    for (int attempt = 0; attempt < 2; ++attempt) {
-      out.clear();
-      int cur = BUF_SRC;
-      bool first = true;
-      for (int a = ndim - 1; a >= 0; --a) {
-        int64_t I = 1, O = 1;
-        for (int b = a + 1; b < ndim; ++b) I *= dims[b];
-        for (int b = 0; b < a; ++b) O *= dims[b];
-        if (dims[a] == 1) continue;
-        const bool foop = first && attempt == 1;
-        int rc = axis(out, O, dims[a], I, cur, foop, false);
-        if (rc) return rc;
-        first = false;
+    out.clear();
+    int cur = BUF_SRC;
+    int a = ndim - 1;
+    // the contiguous axis and its neighbour: two transposing passes when both
+    // lengths have a specialised pass (every store is then a column tile)
+    while (a >= 0 && dims[a] == 1) --a;
+    if (a >= 1) {
+      int b = a - 1;
+      while (b >= 0 && dims[b] == 1) --b;
+      // only when the two axes are adjacent and some outer axis remains to
+      // absorb the buffer parity (the pair itself ends where it started)
+      int outer = 0;
+      for (int c = 0; c < b; ++c) outer += dims[c] > 1;
+      if (b >= 0 && b == a - 1 && outer > 0) {
+        int64_t O = 1;
+        for (int c = 0; c < b; ++c) O *= dims[c];
+        if (transposed_pair(out, O, dims[b], dims[a], cur, other_buf(cur), cur)) a = b - 1;
       }
-      if (out.empty()) {
-        Step cp;
-        cp.kind = ST_COPY;
-        cp.in_buf = BUF_SRC;
-        cp.out_buf = BUF_DST;
-        int64_t t = 1;
-        for (int b = 0; b < ndim; ++b) t *= dims[b];
-        cp.total = t;
-        out.push_back(cp);
-        return 0;
-      }
-      if (cur == BUF_DST) return 0;
     }
-    return set_err(SHAFFT_SM100_ENOTSUP, "planner could not place the result in dst");
+    for (; a >= 0; --a) {
+      int64_t I = 1, O = 1;
+      for (int b = a + 1; b < ndim; ++b) I *= dims[b];
+      for (int b = 0; b < a; ++b) O *= dims[b];
+      if (dims[a] == 1) continue;
+      int rc = axis(out, O, dims[a], I, cur, false, false);
+      if (rc) return rc;
+    }
+    if (out.empty()) {
+      Step cp;
+      cp.kind = ST_COPY;
+      cp.in_buf = BUF_SRC;
+      cp.out_buf = BUF_DST;
+      int64_t t = 1;
+      for (int b = 0; b < ndim; ++b) t *= dims[b];
+      cp.total = t;
+      out.push_back(cp);
+      return 0;
+    }
+    if (out.back().out_buf == BUF_DST) return 0;
+    // Parity fix: let the last in-place step write the other buffer instead,
+    // and exchange src/dst for every step after it.
+    for (int i = (int)out.size() - 1; i >= 0; --i) {
+      Step& st = out[i];
+      const bool user = (st.in_buf == BUF_SRC || st.in_buf == BUF_DST);
+      const bool inplace_pass = st.kind == ST_PASS && user && st.in_buf == st.out_buf;
+      const bool demod = st.kind == ST_BS_DEMOD && (st.out_buf == BUF_SRC || st.out_buf == BUF_DST);
+      if (inplace_pass || demod) {
+        st.out_buf = other_buf(demod ? st.out_buf : st.in_buf);
+        for (size_t j = i + 1; j < out.size(); ++j) {
+          Step& t = out[j];
+          if (t.in_buf == BUF_SRC || t.in_buf == BUF_DST) t.in_buf = other_buf(t.in_buf);
+          if (t.out_buf == BUF_SRC || t.out_buf == BUF_DST) t.out_buf = other_buf(t.out_buf);
+        }
+        if (out.back().out_buf == BUF_DST) return 0;
+        break;
+      }
+      // a Bluestein block writes its result to its input buffer through
+      // scratch; the demodulate step above handles it
+    }
+    // last resort: copy
+    Step cp;
+    cp.kind = ST_COPY;
+    cp.in_buf = out.back().out_buf;
+    cp.out_buf = BUF_DST;
+    int64_t t = 1;
+    for (int b = 0; b < ndim; ++b) t *= dims[b];
+    cp.total = t;
+    out.push_back(cp);
+    return 0;
   }
 };
 
@@ -560,6 +685,10 @@ struct Launcher {
       g.tw_shift = nt.shift;
       g.tw_mask = nt.mask;
     }
+    if (st.fast)
+      return check(K::fast(g, st.fast_row != 0, reinterpret_cast<const C*>(in),
+                           reinterpret_cast<C*>(out), tables(p, st), s),
+                   "fast fft pass");
     return check(K::pass(g, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), tables(p, st),
                          st.smem, s),
                  "fft pass");
@@ -660,11 +789,11 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
       snprintf(b, sizeof(b),
                "{\"kind\":\"pass\",\"L\":%d,\"radices\":[%s],\"W\":%d,\"in\":\"%s\",\"out\":\"%s\","
                "\"in_row\":%d,\"out_row\":%d,\"tiles\":%lld,\"smem\":%zu,\"twiddle\":%d,"
-               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld}",
+               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d}",
                st.g.L, rad.c_str(), st.g.W, buf_name(st.in_buf), buf_name(st.out_buf), st.g.in_row,
                st.g.out_row, (long long)st.g.ntiles, st.smem, st.g.tw_mode, (long long)st.g.ext[0],
                (long long)st.g.ext[1], (long long)st.g.ext[2], (long long)st.g.ext[3],
-               (long long)st.g.sn_in, (long long)st.g.sk_out);
+               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast);
     } else {
       const char* k = st.kind == ST_BS_MOD    ? "bluestein_modulate"
                       : st.kind == ST_BS_MULH ? "bluestein_multiply"
