@@ -62,21 +62,53 @@ struct Chunk {
 
 __device__ __forceinline__ int swz(int p, int c) { return p * 8 + (c ^ (p & 7)); }
 
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW>
-__global__ void __launch_bounds__(NT)
-    k_fft_fast(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
-               typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+// Streaming (evict-first) global accesses for the tensor, so that the small
+// twiddle table stays resident in L1; twiddles use the read-only path.
+template <typename C>
+__device__ __forceinline__ C ld_stream(const C* p);
+template <>
+__device__ __forceinline__ float2 ld_stream<float2>(const float2* p) { return __ldcs(p); }
+template <>
+__device__ __forceinline__ double2 ld_stream<double2>(const double2* p) { return __ldcs(p); }
+__device__ __forceinline__ float4 ld_chunk(const void* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void st_chunk(void* p, float4 v) { __stcs(reinterpret_cast<float4*>(p), v); }
+template <typename C>
+__device__ __forceinline__ C ld_tw(const C* p) { return __ldg(p); }
+
+// Cache policy of a tile's HBM traffic.
+//   LD_STREAM : input read once from HBM, evict-first in L1/L2
+//   LD_L2     : input produced moments ago by another CTA; read at L2 only
+enum TileLoad : int { LD_STREAM = 0, LD_L2 = 1 };
+//   ST_STREAM : final output, evict-first
+//   ST_KEEP   : intermediate that another CTA reads next; default policy
+enum TileStore : int { ST_STREAM = 0, ST_KEEP = 1 };
+
+template <typename C>
+__device__ __forceinline__ C ld_l2(const C* p);
+template <>
+__device__ __forceinline__ float2 ld_l2<float2>(const float2* p) { return __ldcg(p); }
+template <>
+__device__ __forceinline__ double2 ld_l2<double2>(const double2* p) { return __ldcg(p); }
+
+// Drop a 128-byte line from L2 without writing it back (its contents were
+// consumed and will be overwritten before they are read again).
+__device__ __forceinline__ void discard_line(const void* p) {
+  asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP, int STP, bool DISCARD>
+__device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T>::type* in,
+                                          typename Cx<T>::type* out,
+                                          const PassTables<typename Cx<T>::type>& tb, int64_t tile,
+                                          float4* sm) {
   using C = typename Cx<T>::type;
   using Cfg = FastCfg<L, R0, R1, R2, NT>;
   constexpr int VW = ChunkT<T>::VW;
   constexpr int W = 8 * VW;
   constexpr int S = Cfg::S;
   constexpr int RL = (S == 3) ? R2 : R1;  // radix of the last stage
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float4* sm = reinterpret_cast<float4*>(smem_raw);  // L rows x 8 chunks of 16 bytes
 
   const int tid = threadIdx.x;
-  int64_t tile = blockIdx.x;
   const int64_t tw = tile % g.tiles_w;
   int64_t rest = tile / g.tiles_w;
   const int64_t i1 = rest % g.ext[1];
@@ -116,10 +148,12 @@ __global__ void __launch_bounds__(NT)
         if (IN_ROW) {
 #pragma unroll
           for (int e = 0; e < VW; ++e)
-            v[b][r][e] = in[bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n];
+            v[b][r][e] = (LDP == LD_L2) ? ld_l2(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n)
+                                        : ld_stream(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n);
         } else {
-          const Chunk<C, VW> ch =
-              *reinterpret_cast<const Chunk<C, VW>*>(in + bin + bc[b] * VW + (int64_t)n * g.sn_in);
+          const void* src = in + bin + bc[b] * VW + (int64_t)n * g.sn_in;
+          float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
+          const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
           for (int e = 0; e < VW; ++e) v[b][r][e] = ch.v[e];
         }
@@ -138,7 +172,7 @@ __global__ void __launch_bounds__(NT)
         dft<R0>(x);
         if (bj[b] != 0) {
 #pragma unroll
-          for (int r = 1; r < R0; ++r) x[r] = cmul(x[r], tb.twL[bj[b] * r]);
+          for (int r = 1; r < R0; ++r) x[r] = cmul(x[r], ld_tw(tb.twL + bj[b] * r));
         }
 #pragma unroll
         for (int r = 0; r < R0; ++r) v[b][r][e] = x[r];
@@ -154,6 +188,18 @@ __global__ void __launch_bounds__(NT)
     }
   }
   __syncthreads();
+  if constexpr (DISCARD) {
+    // every input line of this tile has been consumed: W rows (IN_ROW) of L
+    // points, or L rows of one 128-byte column chunk
+    constexpr int LINE = 128 / (int)sizeof(C);
+    if constexpr (IN_ROW) {
+      constexpr int LPR = L / LINE;  // lines per input row
+      for (int l = tid; l < W * LPR; l += NT)
+        discard_line(in + bin + (int64_t)(l / LPR) * g.sin[0] + (l % LPR) * LINE);
+    } else {
+      for (int l = tid; l < L; l += NT) discard_line(in + bin + (int64_t)l * g.sn_in);
+    }
+  }
 
   // ---------------- phase B: middle stage (3-stage plans) ----------------
   if constexpr (S == 3) {
@@ -182,7 +228,7 @@ __global__ void __launch_bounds__(NT)
         dft<R1>(y);
         if (j != 0) {
 #pragma unroll
-          for (int r = 1; r < R1; ++r) y[r] = cmul(y[r], tb.twL[j * r * R0]);
+          for (int r = 1; r < R1; ++r) y[r] = cmul(y[r], ld_tw(tb.twL + j * r * R0));
         }
 #pragma unroll
         for (int r = 0; r < R1; ++r) x[r][e] = y[r];
@@ -243,15 +289,64 @@ __global__ void __launch_bounds__(NT)
           if (g.tw_mode == TW_POST) {
             const int64_t t = (g.tw_dim == 0) ? (w0 + c * VW + e) : tconst;
             const int64_t m = (int64_t)k * t;
-            y = cmul(y, cmul(tb.tw_hi[m >> g.tw_shift], tb.tw_lo[m & g.tw_mask]));
+            y = cmul(y, cmul(ld_tw(tb.tw_hi + (m >> g.tw_shift)), ld_tw(tb.tw_lo + (m & g.tw_mask))));
           }
           if (g.scale != 1.0) y = cscale(y, scale);
           if (g.conj_out) y.y = -y.y;
           ch.v[e] = y;
         }
-        *reinterpret_cast<Chunk<C, VW>*>(out + bout + c * VW + (int64_t)k * g.sk_out) = ch;
+        float4* dstp = reinterpret_cast<float4*>(out + bout + c * VW + (int64_t)k * g.sk_out);
+        if (STP == ST_STREAM)
+          st_chunk(dstp, *reinterpret_cast<float4*>(&ch));
+        else
+          *dstp = *reinterpret_cast<float4*>(&ch);
       }
     }
+  }
+}
+
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW>
+__global__ void __launch_bounds__(NT)
+    k_fft_fast(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
+               typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  fast_tile<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false>(
+      g, in, out, tb, blockIdx.x, reinterpret_cast<float4*>(smem_raw));
+}
+
+// Two axes of a stack of square L x L planes in one HBM pass.  One thread
+// block cluster of `cl` CTAs owns a plane (cluster index = plane):
+//   X phase: row tiles of `src` -> transposed column tiles of `mid`
+//            (mid keeps the default L2 policy; the plane, 2 MiB for
+//            512^2 complex64, stays resident in the 126 MB L2);
+//   cluster barrier (release/acquire at cluster scope after a gpu fence);
+//   Y phase: row tiles of `mid` read at L2 -> natural-order column tiles of
+//            `dst`; each consumed `mid` line is discarded from L2 so the
+//            intermediate never reaches HBM.
+// mid must not alias src or dst; src may alias dst (the X phase has consumed
+// the whole plane before the Y phase writes it).
+template <typename T, int L, int R0, int R1, int R2, int NT>
+__global__ void __launch_bounds__(NT)
+    k_fft_plane(const __grid_constant__ PassGeom gx, const __grid_constant__ PassGeom gy,
+                const typename Cx<T>::type* src, typename Cx<T>::type* mid,
+                typename Cx<T>::type* dst, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float4* sm = reinterpret_cast<float4*>(smem_raw);
+  unsigned rank, nrank, cid;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(nrank));
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(cid));
+  const int64_t plane = cid;
+  const int64_t tx = gx.tiles_w, ty = gy.tiles_w;
+  for (int64_t t = rank; t < tx; t += nrank) {
+    fast_tile<T, L, R0, R1, R2, NT, true, LD_STREAM, ST_KEEP, false>(gx, src, mid, tb, plane * tx + t, sm);
+    __syncthreads();
+  }
+  __threadfence();
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+  for (int64_t t = rank; t < ty; t += nrank) {
+    fast_tile<T, L, R0, R1, R2, NT, true, LD_L2, ST_STREAM, true>(gy, mid, dst, tb, plane * ty + t, sm);
+    __syncthreads();
   }
 }
 

@@ -34,6 +34,35 @@ struct FastTable;
   X(256, 8, 8, 4, 128)          \
   X(512, 8, 8, 8, 256)
 
+
+#define SHAFFT_PLANE_LIST_F32(X) \
+  X(128, 8, 4, 4, 128)           \
+  X(256, 8, 8, 4, 256)           \
+  X(512, 8, 8, 8, 256)           \
+  X(1024, 8, 8, 16, 512)
+#define SHAFFT_PLANE_LIST_F64(X) \
+  X(128, 8, 4, 4, 128)           \
+  X(256, 8, 8, 4, 128)           \
+  X(512, 8, 8, 8, 256)
+
+template <typename KernelT, typename... Args>
+static cudaError_t launch_cluster(KernelT kernel, int planes, int cluster, int threads, size_t smem,
+                                  cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(planes * cluster), 1, 1);
+  cfg.blockDim = dim3((unsigned)threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <typename T>
 static cudaError_t fast_attr_all();
 
@@ -50,6 +79,12 @@ cudaError_t fast_attr_all<float>() {
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
   SHAFFT_FAST_LIST_F32(SHAFFT_ATTR)
 #undef SHAFFT_ATTR
+#define SHAFFT_PATTR(L, A, B, C_, NT)                                                            \
+  if (e == cudaSuccess)                                                                          \
+    e = cudaFuncSetAttribute(k_fft_plane<float, L, A, B, C_, NT>,                                \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+  SHAFFT_PLANE_LIST_F32(SHAFFT_PATTR)
+#undef SHAFFT_PATTR
   return e;
 }
 #endif
@@ -66,6 +101,12 @@ cudaError_t fast_attr_all<double>() {
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
   SHAFFT_FAST_LIST_F64(SHAFFT_ATTR)
 #undef SHAFFT_ATTR
+#define SHAFFT_PATTR(L, A, B, C_, NT)                                                            \
+  if (e == cudaSuccess)                                                                          \
+    e = cudaFuncSetAttribute(k_fft_plane<double, L, A, B, C_, NT>,                               \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+  SHAFFT_PLANE_LIST_F64(SHAFFT_PATTR)
+#undef SHAFFT_PATTR
   return e;
 }
 
@@ -150,6 +191,56 @@ cudaError_t Launch<double>::fast(const PassGeom& g, bool in_row, const C* in, C*
       k_fft_fast<double, L_, A, B, C_, NT, false><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);  \
     return cudaGetLastError();
     SHAFFT_FAST_LIST_F64(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return cudaErrorNotSupported;
+  }
+}
+#endif
+
+#ifdef SHAFFT_INSTANTIATE_F32
+template <>
+bool Launch<float>::plane_supported(int L) {
+  switch (L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
+    SHAFFT_PLANE_LIST_F32(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return false;
+  }
+}
+template <>
+cudaError_t Launch<float>::plane(const PassGeom& gx, const PassGeom& gy, const C* src, C* mid, C* dst,
+                               const PassTables<C>& tb, int planes, int cluster, cudaStream_t s) {
+  switch (gx.L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT)                                                            \
+  case L_:                                                                                       \
+    return launch_cluster(k_fft_plane<float, L_, A, B, C_, NT>, planes, cluster, NT, L_ * 128, s,  \
+                          gx, gy, src, mid, dst, tb);
+    SHAFFT_PLANE_LIST_F32(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return cudaErrorNotSupported;
+  }
+}
+#endif
+
+#ifdef SHAFFT_INSTANTIATE_F64
+template <>
+bool Launch<double>::plane_supported(int L) {
+  switch (L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
+    SHAFFT_PLANE_LIST_F64(SHAFFT_CASE)
+#undef SHAFFT_CASE
+    default: return false;
+  }
+}
+template <>
+cudaError_t Launch<double>::plane(const PassGeom& gx, const PassGeom& gy, const C* src, C* mid, C* dst,
+                               const PassTables<C>& tb, int planes, int cluster, cudaStream_t s) {
+  switch (gx.L) {
+#define SHAFFT_CASE(L_, A, B, C_, NT)                                                            \
+  case L_:                                                                                       \
+    return launch_cluster(k_fft_plane<double, L_, A, B, C_, NT>, planes, cluster, NT, L_ * 128, s,  \
+                          gx, gy, src, mid, dst, tb);
+    SHAFFT_PLANE_LIST_F64(SHAFFT_CASE)
 #undef SHAFFT_CASE
     default: return cudaErrorNotSupported;
   }

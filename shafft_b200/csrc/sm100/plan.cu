@@ -26,6 +26,7 @@
 #include <stdarg.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -63,7 +64,7 @@ static int set_err(int code, const char* fmt, ...) {
     }                                                                                    \
   } while (0)
 
-enum StepKind : int { ST_PASS = 0, ST_BS_MOD, ST_BS_MULH, ST_BS_DEMOD, ST_COPY };
+enum StepKind : int { ST_PASS = 0, ST_BS_MOD, ST_BS_MULH, ST_BS_DEMOD, ST_COPY, ST_PLANE };
 enum BufId : int { BUF_SRC = 0, BUF_DST = 1, BUF_S0 = 2, BUF_S1 = 3 };
 
 static int other_buf(int b) {
@@ -89,6 +90,11 @@ struct Step {
   size_t smem = 0;
   int fast = 0;      // 1: specialised k_fft_fast pass (compile-time L)
   int fast_row = 0;  // specialised pass reads row tiles (transposing)
+  // ST_PLANE: g = X phase (src -> mid), g2 = Y phase (mid -> out)
+  PassGeom g2{};
+  int mid_buf = BUF_DST;
+  int cluster = 8;
+  int64_t planes = 0;
 };
 
 struct LTable {
@@ -148,7 +154,12 @@ struct Planner {
   size_t table_bytes = 0;
   int64_t scratch_elems = 0;
 
-  explicit Planner(int prec) : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {}
+  explicit Planner(int prec) : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {
+    if (const char* e = getenv("SHAFFT_SM100_PLANE_CLUSTER")) {
+      const int v = atoi(e);
+      plane_cluster = (v == 0) ? -1 : v;  // 0 disables the fused plane pass
+    }
+  }
 
   // specialised-pass eligibility: length, tile width and 16-byte alignment
   int fast_w() const { return precision ? 8 : 16; }
@@ -279,6 +290,33 @@ struct Planner {
     }
     out.push_back(st);
   }
+
+  bool plane_len(int64_t L) const {
+    if (L > 1 << 20) return false;
+    return precision ? Launch<double>::plane_supported((int)L) : Launch<float>::plane_supported((int)L);
+  }
+
+  // The last two axes of a stack of O square L x L planes in one HBM pass
+  // (k_fft_plane): buf -> (mid = other(buf)) -> buf.
+  bool plane_step(std::vector<Step>& out, int64_t O, int64_t L, int buf) {
+    if (plane_cluster < 1 || plane_cluster > 8 || !plane_len(L) || L % fast_w() || O < 16) return false;
+    std::vector<Step> tmp;
+    if (!transposed_pair(tmp, O, L, L, buf, other_buf(buf), buf)) return false;
+    Step st;
+    st.kind = ST_PLANE;
+    st.g = tmp[0].g;
+    st.g2 = tmp[1].g;
+    st.in_buf = buf;
+    st.mid_buf = other_buf(buf);
+    st.out_buf = buf;
+    st.tabL = tmp[0].tabL;
+    st.smem = (size_t)L * 128;
+    st.planes = O;
+    st.cluster = plane_cluster;
+    out.push_back(st);
+    return true;
+  }
+  int plane_cluster = -1;  // fused plane pass off unless SHAFFT_SM100_PLANE_CLUSTER selects a cluster size
 
   // The last two axes (A = rows, Lr = contiguous) as two transposing passes:
   // rows of Lr -> [o][kL][a] in `mid`, then rows of A -> [o][ka][kL] in
@@ -534,7 +572,10 @@ struct Planner {
       if (b >= 0 && b == a - 1 && outer > 0) {
         int64_t O = 1;
         for (int c = 0; c < b; ++c) O *= dims[c];
-        if (transposed_pair(out, O, dims[b], dims[a], cur, other_buf(cur), cur)) a = b - 1;
+        if (dims[b] == dims[a] && plane_step(out, O, dims[a], cur))
+          a = b - 1;
+        else if (transposed_pair(out, O, dims[b], dims[a], cur, other_buf(cur), cur))
+          a = b - 1;
       }
     }
     for (; a >= 0; --a) {
@@ -570,6 +611,7 @@ struct Planner {
           Step& t = out[j];
           if (t.in_buf == BUF_SRC || t.in_buf == BUF_DST) t.in_buf = other_buf(t.in_buf);
           if (t.out_buf == BUF_SRC || t.out_buf == BUF_DST) t.out_buf = other_buf(t.out_buf);
+          if (t.kind == ST_PLANE) t.mid_buf = other_buf(t.mid_buf);
         }
         if (out.back().out_buf == BUF_DST) return 0;
         break;
@@ -694,6 +736,22 @@ struct Launcher {
                  "fft pass");
   }
 
+  static int plane(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* mid, void* out,
+                   bool conj_in, bool conj_out, double scale, cudaStream_t s) {
+    int rc = init_once();
+    if (rc) return rc;
+    PassGeom gx = st.g, gy = st.g2;
+    gx.conj_in = conj_in;
+    gx.conj_out = 0;
+    gx.scale = 1.0;
+    gy.conj_in = 0;
+    gy.conj_out = conj_out;
+    gy.scale = scale;
+    return check(K::plane(gx, gy, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(mid),
+                          reinterpret_cast<C*>(out), tables(p, st), (int)st.planes, st.cluster, s),
+                 "plane pass");
+  }
+
   static int elementwise(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* out,
                          bool conj_in, bool conj_out, double scale, cudaStream_t s) {
     const C* cin = reinterpret_cast<const C*>(in);
@@ -727,6 +785,8 @@ struct Launcher {
       int rc;
       if (st.kind == ST_PASS)
         rc = pass(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
+      else if (st.kind == ST_PLANE)
+        rc = plane(p, st, bufs[st.in_buf], bufs[st.mid_buf], bufs[st.out_buf], cin, cout, sc, s);
       else
         rc = elementwise(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
       if (rc) return rc;
@@ -783,7 +843,12 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
   for (size_t i = 0; i < steps.size(); ++i) {
     const Step& st = steps[i];
     char b[768];
-    if (st.kind == ST_PASS) {
+    if (st.kind == ST_PLANE) {
+      snprintf(b, sizeof(b),
+               "{\"kind\":\"plane\",\"L\":%d,\"planes\":%lld,\"cluster\":%d,\"in\":\"%s\",\"mid\":\"%s\",\"out\":\"%s\",\"fast\":1}",
+               st.g.L, (long long)st.planes, st.cluster, buf_name(st.in_buf), buf_name(st.mid_buf),
+               buf_name(st.out_buf));
+    } else if (st.kind == ST_PASS) {
       std::string rad;
       for (int r = 0; r < st.g.nst; ++r) rad += (r ? "," : "") + std::to_string(st.g.rad[r]);
       snprintf(b, sizeof(b),
@@ -946,6 +1011,7 @@ int64_t shafft_sm100_step_bytes(shafft_sm100_plan plan, int step) {
   if (!plan || step < 0 || step >= (int)plan->steps.size()) return 0;
   const Step& st = plan->steps[step];
   const int64_t es = plan->precision ? 16 : 8;
+  if (st.kind == ST_PLANE) return 2 * st.planes * st.g.L * st.g.L * es;
   if (st.kind == ST_PASS) {
     int64_t n = (int64_t)st.g.L;
     for (int d = 0; d < 4; ++d) n *= st.g.ext[d];
