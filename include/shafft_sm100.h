@@ -118,6 +118,29 @@ int shafft_sm100_stream_sync(void* stream);
 /* Name of the current CUDA device. */
 int shafft_sm100_device_name(char* buf, int buflen);
 
+/* Allocation-free 1-D C2C transform (no counterpart in the reference).
+ *
+ * For callers that cannot call cudaMalloc where they need the transform --
+ * code running under an allocator lock, inside a framework callback that
+ * forbids allocation, or within a fixed device-memory budget reserved up
+ * front.  It takes only the caller's input and output device buffers of n
+ * complex elements (in == out is allowed) and computes the unnormalised
+ * length-n DFT (direction 0 forward, 1 backward) times `scale`, by
+ * Bluestein's chirp-z method over a power-of-two convolution, for any n in
+ * 1..2048.  Larger n is rejected with SHAFFT_SM100_EINVAL.
+ *
+ * All device state (chirp, kernel spectrum, twiddle and digit tables, two
+ * convolution rows) lives in one file-scope __device__ array of about
+ * 304 KiB that every device loading this library keeps until the process
+ * exits.  Each call regenerates what it reads, so results do not depend on
+ * earlier calls, but all calls on a device share the array: calls whose work
+ * overlaps on the GPU race and corrupt each other -- issue them in order on
+ * one stream.  The first call on a device looks the array's address up with
+ * cudaGetSymbolAddress; make that first call before any stream capture.
+ * Asynchronous on `stream` (cudaStream_t, NULL = legacy default stream). */
+int shafft_sm100_bluestein_noalloc(const void* in, void* out, int64_t n, int precision,
+                                   int direction, double scale, void* stream);
+
 /* Last CUDA runtime error code seen by this library on this thread. */
 int shafft_sm100_last_cuda_error(void);
 

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(kThreads)
     k_fft_pass(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
                typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
   using C = typename Cx<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
   constexpr RadixPlan P = radix_plan(LS > 0 ? LS : 1);
   const int L = LS ? LS : g.L;

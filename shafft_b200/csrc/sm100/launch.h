@@ -9,6 +9,10 @@
 
 namespace shafft_sm100 {
 
+// Record `msg` as this thread's last error of the library (returned by
+// shafft_sm100_last_error_message) and return `code`.
+int report_error(int code, const char* msg);
+
 template <typename T>
 struct Vec2;
 template <>

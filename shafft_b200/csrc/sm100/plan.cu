@@ -54,6 +54,11 @@ static int set_err(int code, const char* fmt, ...) {
   return code;
 }
 
+int report_error(int code, const char* msg) {
+  snprintf(g_last_msg, sizeof(g_last_msg), "%s", msg);
+  return code;
+}
+
 #define CUDA_TRY(expr)                                                                   \
   do {                                                                                   \
     cudaError_t e_ = (expr);                                                             \
