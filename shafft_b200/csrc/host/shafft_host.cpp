@@ -134,6 +134,8 @@ public:
     if (rc) return backend_fail(rc, "execute");
     rc = shafft_sm100_stream_sync(stream);
     if (rc) return backend_fail(rc, "stream synchronize");
+    rc = shafft_sm100_plan_status(kplan);
+    if (rc) return backend_fail(rc, "execute");
     std::swap(data, work);
     normExp = normalized ? 0 : normExp + 1;
     layoutState = (dir == FFTDirection::FORWARD) ? 1 : 0;

@@ -82,6 +82,13 @@ enum TileLoad : int { LD_STREAM = 0, LD_L2 = 1 };
 //   ST_STREAM : final output, evict-first
 //   ST_KEEP   : intermediate that another CTA reads next; default policy
 enum TileStore : int { ST_STREAM = 0, ST_KEEP = 1 };
+// LDP/STP = POLICY_RUNTIME: policies (and the L2 discard) come from the
+// runtime `pol` argument of fast_tile, so one instantiation serves several
+// tile kinds.
+constexpr int POLICY_RUNTIME = 2;
+struct TilePolicy {
+  int ld, st, discard;
+};
 
 template <typename C>
 __device__ __forceinline__ C ld_l2(const C* p);
@@ -96,12 +103,15 @@ __device__ __forceinline__ void discard_line(const void* p) {
   asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
 }
 
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP, int STP, bool DISCARD>
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_>
 __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T>::type* in,
                                           typename Cx<T>::type* out,
                                           const PassTables<typename Cx<T>::type>& tb, int64_t tile,
-                                          float4* sm) {
+                                          float4* sm, TilePolicy pol = TilePolicy{0, 0, 0}) {
   using C = typename Cx<T>::type;
+  const int LDP = (LDP_ == POLICY_RUNTIME) ? pol.ld : LDP_;
+  const int STP = (STP_ == POLICY_RUNTIME) ? pol.st : STP_;
+  const bool DISCARD = (LDP_ == POLICY_RUNTIME) ? (pol.discard != 0) : DISCARD_;
   using Cfg = FastCfg<L, R0, R1, R2, NT>;
   constexpr int VW = ChunkT<T>::VW;
   constexpr int W = 8 * VW;
@@ -188,7 +198,7 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
     }
   }
   __syncthreads();
-  if constexpr (DISCARD) {
+  if (DISCARD) {
     // every input line of this tile has been consumed: W rows (IN_ROW) of L
     // points, or L rows of one 128-byte column chunk
     constexpr int LINE = 128 / (int)sizeof(C);
@@ -314,39 +324,112 @@ __global__ void __launch_bounds__(NT)
       g, in, out, tb, blockIdx.x, reinterpret_cast<float4*>(smem_raw));
 }
 
-// Two axes of a stack of square L x L planes in one HBM pass.  One thread
-// block cluster of `cl` CTAs owns a plane (cluster index = plane):
-//   X phase: row tiles of `src` -> transposed column tiles of `mid`
-//            (mid keeps the default L2 policy; the plane, 2 MiB for
-//            512^2 complex64, stays resident in the 126 MB L2);
-//   cluster barrier (release/acquire at cluster scope after a gpu fence);
-//   Y phase: row tiles of `mid` read at L2 -> natural-order column tiles of
-//            `dst`; each consumed `mid` line is discarded from L2 so the
+// Two axes of a stack of square L x L planes in one HBM pass, as a
+// persistent dataflow kernel.  Control words (zeroed before each launch):
+// 64-bit ticket counter at ctl[0..1], error flag ctl[2], per-plane counters
+// ctl[4 + plane].  Work items ("tickets", claimed in increasing order) are
+// the X tiles of plane g followed by the Y tiles of plane g - lag:
+//   X tile : row tiles of `src` -> transposed column tiles of `mid` (default
+//            L2 policy: the plane is read back moments later), then the
+//            plane's counter ctl[4 + plane] is incremented (after a gpu fence);
+//   Y tile : waits until that counter reaches the plane's X-tile count, then
+//            reads row tiles of `mid` at L2 -> natural-order column tiles of
+//            `dst`, and discards the consumed `mid` lines from L2 so the
 //            intermediate never reaches HBM.
-// mid must not alias src or dst; src may alias dst (the X phase has consumed
-// the whole plane before the Y phase writes it).
+// Only about lag + (resident CTAs / tiles per plane) planes are in flight, so
+// their intermediates (2 MiB per 512^2 complex64 plane) stay inside L2.
+// Progress: every X ticket of a plane precedes every Y ticket of that plane,
+// X items never wait, and a ticket is only claimed by a running CTA, so each
+// wait ends.  The wait is still bounded: after kFlowSpinLimit polls the CTA
+// sets ctl[2] = 1 (reported by the host as an error) and continues.
+// mid must not alias src or dst; src may alias dst.
+constexpr unsigned kFlowSpinLimit = 1u << 22;
+
+struct FlowShape {
+  int64_t planes, tx, ty, lag;
+  TilePolicy xpol, ypol;  // cache policies of the X and Y tiles
+};
+
+// ticket -> (is_y, plane, tile within plane); returns false past the end
+__device__ __forceinline__ bool flow_decode(const FlowShape& f, int64_t t, bool& is_y, int64_t& plane,
+                                            int64_t& tile) {
+  const int64_t P = f.planes, D = f.lag, tx = f.tx, ty = f.ty;
+  const int64_t A = D * tx, Bm = (P - D) * (tx + ty);
+  if (t < A) {
+    is_y = false;
+    plane = t / tx;
+    tile = t % tx;
+    return true;
+  }
+  if (t < A + Bm) {
+    const int64_t u = t - A, g = D + u / (tx + ty), r = u % (tx + ty);
+    if (r < tx) {
+      is_y = false;
+      plane = g;
+      tile = r;
+    } else {
+      is_y = true;
+      plane = g - D;
+      tile = r - tx;
+    }
+    return true;
+  }
+  const int64_t u = t - A - Bm;
+  if (u >= D * ty) return false;
+  is_y = true;
+  plane = P - D + u / ty;
+  tile = u % ty;
+  return true;
+}
+
 template <typename T, int L, int R0, int R1, int R2, int NT>
-__global__ void __launch_bounds__(NT)
-    k_fft_plane(const __grid_constant__ PassGeom gx, const __grid_constant__ PassGeom gy,
-                const typename Cx<T>::type* src, typename Cx<T>::type* mid,
-                typename Cx<T>::type* dst, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+__global__ void __launch_bounds__(NT, (L * 128 <= 64 * 1024) ? 3 : 1)
+    k_fft_plane_flow(const __grid_constant__ PassGeom gx, const __grid_constant__ PassGeom gy,
+                     const typename Cx<T>::type* src, typename Cx<T>::type* mid,
+                     typename Cx<T>::type* dst,
+                     const __grid_constant__ PassTables<typename Cx<T>::type> tb, int* ctl,
+                     const FlowShape f) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float4* sm = reinterpret_cast<float4*>(smem_raw);
-  unsigned rank, nrank, cid;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
-  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(nrank));
-  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(cid));
-  const int64_t plane = cid;
-  const int64_t tx = gx.tiles_w, ty = gy.tiles_w;
-  for (int64_t t = rank; t < tx; t += nrank) {
-    fast_tile<T, L, R0, R1, R2, NT, true, LD_STREAM, ST_KEEP, false>(gx, src, mid, tb, plane * tx + t, sm);
-    __syncthreads();
-  }
-  __threadfence();
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-  for (int64_t t = rank; t < ty; t += nrank) {
-    fast_tile<T, L, R0, R1, R2, NT, true, LD_L2, ST_STREAM, true>(gy, mid, dst, tb, plane * ty + t, sm);
-    __syncthreads();
+  // two ticket slots after the tile (dynamic shared memory is L*128 + 128 bytes)
+  volatile long long* s_tk = reinterpret_cast<volatile long long*>(smem_raw + L * 128);
+  unsigned long long* ticket = reinterpret_cast<unsigned long long*>(ctl);
+  if (threadIdx.x == 0) s_tk[0] = (long long)atomicAdd(ticket, 1ull);
+  __syncthreads();
+  for (int slot = 0;; slot ^= 1) {
+    const int64_t t = s_tk[slot];
+    // claim the next ticket now; it is published by this item's last barrier
+    if (threadIdx.x == 0) s_tk[slot ^ 1] = (long long)atomicAdd(ticket, 1ull);
+    bool is_y;
+    int64_t plane, tile;
+    if (!flow_decode(f, t, is_y, plane, tile)) break;
+    if (!is_y) {
+      fast_tile<T, L, R0, R1, R2, NT, true, POLICY_RUNTIME, POLICY_RUNTIME, false>(
+          gx, src, mid, tb, plane * f.tx + tile, sm, f.xpol);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctl + 4 + plane, 1);
+      }
+    } else {
+      if (threadIdx.x == 0) {
+        unsigned it = 0;
+        for (;;) {
+          int v;
+          asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(ctl + 4 + plane) : "memory");
+          if (v >= f.tx) break;
+          if (++it > kFlowSpinLimit) {
+            atomicExch(ctl + 2, 1);
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __syncthreads();
+      fast_tile<T, L, R0, R1, R2, NT, true, POLICY_RUNTIME, POLICY_RUNTIME, false>(
+          gy, mid, dst, tb, plane * f.ty + tile, sm, f.ypol);
+      __syncthreads();
+    }
   }
 }
 

@@ -38,9 +38,10 @@ struct Launch {
                           const PassTables<C>& tb, cudaStream_t s);
   static bool fast_supported(int L);
   static int fast_threads(int L);
-  // fused two-axis pass over a stack of square L x L planes (see k_fft_plane)
+  // fused two-axis pass over a stack of square L x L planes (see
+  // k_fft_plane_flow); ctl holds 4 + planes ints of plan-owned device memory
   static cudaError_t plane(const PassGeom& gx, const PassGeom& gy, const C* src, C* mid, C* dst,
-                           const PassTables<C>& tb, int planes, int cluster, cudaStream_t s);
+                           const PassTables<C>& tb, int planes, int* ctl, int lag, cudaStream_t s);
   static bool plane_supported(int L);
   static cudaError_t scale_copy(const C* src, C* dst, int64_t n, T factor, int conj, cudaStream_t s);
   static cudaError_t bs_modulate(const C* src, C* dst, int64_t L, int64_t M, int64_t I,
@@ -69,11 +70,11 @@ bool Launch<double>::plane_supported(int L);
 template <>
 cudaError_t Launch<float>::plane(const PassGeom& gx, const PassGeom& gy, const float2* src,
                                  float2* mid, float2* dst, const PassTables<float2>& tb, int planes,
-                                 int cluster, cudaStream_t s);
+                                 int* ctl, int lag, cudaStream_t s);
 template <>
 cudaError_t Launch<double>::plane(const PassGeom& gx, const PassGeom& gy, const double2* src,
                                   double2* mid, double2* dst, const PassTables<double2>& tb,
-                                  int planes, int cluster, cudaStream_t s);
+                                  int planes, int* ctl, int lag, cudaStream_t s);
 template <>
 cudaError_t Launch<float>::fast(const PassGeom& g, bool in_row, const float2* in, float2* out,
                                 const PassTables<float2>& tb, cudaStream_t s);

@@ -1,6 +1,9 @@
 // Definitions of Launch<T> (see launch.h); included by launch_f32.cu and
-// launch_f64.cu only.
+// launch_f64.cu only (each defines SHAFFT_INSTANTIATE_F32 or _F64).
 #pragma once
+#include <stdio.h>
+#include <stdlib.h>
+
 #include <algorithm>
 
 #include "fast.cuh"
@@ -16,8 +19,6 @@ static inline unsigned ew_grid(int64_t n) {
 
 // Compile-time radix plans of the specialised passes: (L, R0, R1, R2, threads).
 // Every stage gives each thread a whole number of 16-byte-chunk butterflies.
-template <typename T>
-struct FastTable;
 #define SHAFFT_FAST_LIST_F32(X) \
   X(16, 4, 4, 1, 32)            \
   X(32, 8, 4, 1, 32)            \
@@ -34,7 +35,7 @@ struct FastTable;
   X(256, 8, 8, 4, 128)          \
   X(512, 8, 8, 8, 256)
 
-
+// Lengths with a fused two-axis plane kernel (k_fft_plane_flow).
 #define SHAFFT_PLANE_LIST_F32(X) \
   X(128, 8, 4, 4, 128)           \
   X(256, 8, 8, 4, 256)           \
@@ -45,71 +46,139 @@ struct FastTable;
   X(256, 8, 8, 4, 128)           \
   X(512, 8, 8, 8, 256)
 
-template <typename KernelT, typename... Args>
-static cudaError_t launch_cluster(KernelT kernel, int planes, int cluster, int threads, size_t smem,
-                                  cudaStream_t s, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(planes * cluster), 1, 1);
-  cfg.blockDim = dim3((unsigned)threads, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)cluster;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, args...);
+// Resident CTAs of `kernel` on the current device.
+template <typename KernelT>
+static unsigned resident_ctas(KernelT kernel, int threads, size_t smem) {
+  int dev = 0, sms = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem) != cudaSuccess ||
+      per < 1)
+    per = 1;
+  return (unsigned)(sms * per);
 }
+
+template <typename T, typename KernelT>
+static cudaError_t launch_flow(KernelT kernel, int threads, size_t smem, const PassGeom& gx,
+                               const PassGeom& gy, const typename Vec2<T>::type* src,
+                               typename Vec2<T>::type* mid, typename Vec2<T>::type* dst,
+                               const PassTables<typename Vec2<T>::type>& tb, int planes, int* ctl,
+                               int lag, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(int) * (size_t)(4 + planes), s);
+  if (e != cudaSuccess) return e;
+  FlowShape f;
+  f.planes = planes;
+  f.tx = gx.tiles_w;
+  f.ty = gy.tiles_w;
+  f.lag = std::max(1, std::min(lag, planes));
+  // cache policies: X tiles keep the intermediate in L2, Y tiles read it at
+  // L2 and discard it; SHAFFT_SM100_FLOW_POLICY="xld,xst,yld,yst,discard"
+  // overrides them (values of TileLoad / TileStore, discard 0/1)
+  f.xpol = TilePolicy{LD_STREAM, ST_KEEP, 0};
+  f.ypol = TilePolicy{LD_L2, ST_STREAM, 1};
+  if (const char* env = getenv("SHAFFT_SM100_FLOW_POLICY")) {
+    int v[5] = {LD_STREAM, ST_KEEP, LD_L2, ST_STREAM, 1};
+    sscanf(env, "%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4]);
+    f.xpol = TilePolicy{v[0], v[1], 0};
+    f.ypol = TilePolicy{v[2], v[3], v[4]};
+  }
+  const unsigned grid = resident_ctas(kernel, threads, smem);
+  kernel<<<grid, threads, smem, s>>>(gx, gy, src, mid, dst, tb, ctl, f);
+  return cudaGetLastError();
+}
+
+#define SHAFFT_DEFINE_PRECISION(TYPE, FASTLIST, PLANELIST)                                       \
+  template <>                                                                                    \
+  cudaError_t fast_attr_all<TYPE>() {                                                            \
+    cudaError_t e = cudaSuccess;                                                                 \
+    FASTLIST(SHAFFT_ATTR_FAST)                                                                   \
+    PLANELIST(SHAFFT_ATTR_PLANE)                                                                 \
+    return e;                                                                                    \
+  }                                                                                              \
+  template <>                                                                                    \
+  bool Launch<TYPE>::fast_supported(int L) {                                                     \
+    switch (L) {                                                                                 \
+      FASTLIST(SHAFFT_CASE_TRUE)                                                                 \
+      default: return false;                                                                     \
+    }                                                                                            \
+  }                                                                                              \
+  template <>                                                                                    \
+  int Launch<TYPE>::fast_threads(int L) {                                                        \
+    switch (L) {                                                                                 \
+      FASTLIST(SHAFFT_CASE_NT)                                                                   \
+      default: return 0;                                                                         \
+    }                                                                                            \
+  }                                                                                              \
+  template <>                                                                                    \
+  bool Launch<TYPE>::plane_supported(int L) {                                                    \
+    switch (L) {                                                                                 \
+      PLANELIST(SHAFFT_CASE_TRUE)                                                                \
+      default: return false;                                                                     \
+    }                                                                                            \
+  }                                                                                              \
+  template <>                                                                                    \
+  cudaError_t Launch<TYPE>::fast(const PassGeom& g, bool in_row, const C* in, C* out,            \
+                                 const PassTables<C>& tb, cudaStream_t s) {                      \
+    const unsigned grid = (unsigned)g.ntiles;                                                    \
+    switch (g.L) {                                                                               \
+      FASTLIST(SHAFFT_CASE_FAST)                                                                 \
+      default: return cudaErrorNotSupported;                                                     \
+    }                                                                                            \
+  }                                                                                              \
+  template <>                                                                                    \
+  cudaError_t Launch<TYPE>::plane(const PassGeom& gx, const PassGeom& gy, const C* src, C* mid,  \
+                                  C* dst, const PassTables<C>& tb, int planes, int* ctl,        \
+                                  int lag, cudaStream_t s) {                                     \
+    switch (gx.L) {                                                                              \
+      PLANELIST(SHAFFT_CASE_PLANE)                                                               \
+      default: return cudaErrorNotSupported;                                                     \
+    }                                                                                            \
+  }
 
 template <typename T>
 static cudaError_t fast_attr_all();
 
+#define SHAFFT_ATTR_FAST(L, A, B, C_, NT)                                                         \
+  if (e == cudaSuccess)                                                                           \
+    e = cudaFuncSetAttribute(k_fft_fast<TYPE_, L, A, B, C_, NT, true>,                            \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);               \
+  if (e == cudaSuccess)                                                                           \
+    e = cudaFuncSetAttribute(k_fft_fast<TYPE_, L, A, B, C_, NT, false>,                           \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+#define SHAFFT_ATTR_PLANE(L, A, B, C_, NT)                                                        \
+  if (e == cudaSuccess)                                                                           \
+    e = cudaFuncSetAttribute(k_fft_plane_flow<TYPE_, L, A, B, C_, NT>,                            \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128 + 128);         \
+  if (e == cudaSuccess)                                                                           \
+    e = cudaFuncSetAttribute(k_fft_plane_flow<TYPE_, L, A, B, C_, NT>,                            \
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+#define SHAFFT_CASE_TRUE(L_, A, B, C_, NT) \
+  case L_:                                 \
+    return true;
+#define SHAFFT_CASE_NT(L_, A, B, C_, NT) \
+  case L_:                               \
+    return NT;
+#define SHAFFT_CASE_FAST(L_, A, B, C_, NT)                                                       \
+  case L_:                                                                                       \
+    if (in_row)                                                                                  \
+      k_fft_fast<TYPE_, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);      \
+    else                                                                                         \
+      k_fft_fast<TYPE_, L_, A, B, C_, NT, false><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);     \
+    return cudaGetLastError();
+#define SHAFFT_CASE_PLANE(L_, A, B, C_, NT)                                                      \
+  case L_:                                                                                       \
+    return launch_flow<TYPE_>(k_fft_plane_flow<TYPE_, L_, A, B, C_, NT>, NT, L_ * 128 + 128, gx, \
+                              gy, src, mid, dst, tb, planes, ctl, lag, s);
+
 #ifdef SHAFFT_INSTANTIATE_F32
-template <>
-cudaError_t fast_attr_all<float>() {
-  cudaError_t e = cudaSuccess;
-#define SHAFFT_ATTR(L, A, B, C_, NT)                                                             \
-  if (e == cudaSuccess)                                                                          \
-    e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, false>,                          \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);              \
-  if (e == cudaSuccess)                                                                          \
-    e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, true>,                           \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
-  SHAFFT_FAST_LIST_F32(SHAFFT_ATTR)
-#undef SHAFFT_ATTR
-#define SHAFFT_PATTR(L, A, B, C_, NT)                                                            \
-  if (e == cudaSuccess)                                                                          \
-    e = cudaFuncSetAttribute(k_fft_plane<float, L, A, B, C_, NT>,                                \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
-  SHAFFT_PLANE_LIST_F32(SHAFFT_PATTR)
-#undef SHAFFT_PATTR
-  return e;
-}
+#define TYPE_ float
+SHAFFT_DEFINE_PRECISION(float, SHAFFT_FAST_LIST_F32, SHAFFT_PLANE_LIST_F32)
+#undef TYPE_
 #endif
 #ifdef SHAFFT_INSTANTIATE_F64
-template <>
-cudaError_t fast_attr_all<double>() {
-  cudaError_t e = cudaSuccess;
-#define SHAFFT_ATTR(L, A, B, C_, NT)                                                             \
-  if (e == cudaSuccess)                                                                          \
-    e = cudaFuncSetAttribute(k_fft_fast<double, L, A, B, C_, NT, false>,                         \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);              \
-  if (e == cudaSuccess)                                                                          \
-    e = cudaFuncSetAttribute(k_fft_fast<double, L, A, B, C_, NT, true>,                          \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
-  SHAFFT_FAST_LIST_F64(SHAFFT_ATTR)
-#undef SHAFFT_ATTR
-#define SHAFFT_PATTR(L, A, B, C_, NT)                                                            \
-  if (e == cudaSuccess)                                                                          \
-    e = cudaFuncSetAttribute(k_fft_plane<double, L, A, B, C_, NT>,                               \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
-  SHAFFT_PLANE_LIST_F64(SHAFFT_PATTR)
-#undef SHAFFT_PATTR
-  return e;
-}
-
+#define TYPE_ double
+SHAFFT_DEFINE_PRECISION(double, SHAFFT_FAST_LIST_F64, SHAFFT_PLANE_LIST_F64)
+#undef TYPE_
 #endif
 
 template <typename T>
@@ -119,133 +188,6 @@ cudaError_t Launch<T>::init() {
   if (e != cudaSuccess) return e;
   return fast_attr_all<T>();
 }
-
-
-
-#ifdef SHAFFT_INSTANTIATE_F32
-template <>
-bool Launch<float>::fast_supported(int L) {
-  switch (L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
-    SHAFFT_FAST_LIST_F32(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return false;
-  }
-}
-template <>
-int Launch<float>::fast_threads(int L) {
-  switch (L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return NT;
-    SHAFFT_FAST_LIST_F32(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return 0;
-  }
-}
-template <>
-cudaError_t Launch<float>::fast(const PassGeom& g, bool in_row, const C* in, C* out,
-                                const PassTables<C>& tb, cudaStream_t s) {
-  const unsigned grid = (unsigned)g.ntiles;
-  switch (g.L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT)                                                          \
-  case L_:                                                                                     \
-    if (in_row)                                                                                \
-      k_fft_fast<float, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);    \
-    else                                                                                       \
-      k_fft_fast<float, L_, A, B, C_, NT, false><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);   \
-    return cudaGetLastError();
-    SHAFFT_FAST_LIST_F32(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return cudaErrorNotSupported;
-  }
-}
-#endif
-#ifdef SHAFFT_INSTANTIATE_F64
-template <>
-bool Launch<double>::fast_supported(int L) {
-  switch (L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
-    SHAFFT_FAST_LIST_F64(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return false;
-  }
-}
-template <>
-int Launch<double>::fast_threads(int L) {
-  switch (L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return NT;
-    SHAFFT_FAST_LIST_F64(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return 0;
-  }
-}
-template <>
-cudaError_t Launch<double>::fast(const PassGeom& g, bool in_row, const C* in, C* out,
-                                 const PassTables<C>& tb, cudaStream_t s) {
-  const unsigned grid = (unsigned)g.ntiles;
-  switch (g.L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT)                                                          \
-  case L_:                                                                                     \
-    if (in_row)                                                                                \
-      k_fft_fast<double, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);   \
-    else                                                                                       \
-      k_fft_fast<double, L_, A, B, C_, NT, false><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);  \
-    return cudaGetLastError();
-    SHAFFT_FAST_LIST_F64(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return cudaErrorNotSupported;
-  }
-}
-#endif
-
-#ifdef SHAFFT_INSTANTIATE_F32
-template <>
-bool Launch<float>::plane_supported(int L) {
-  switch (L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
-    SHAFFT_PLANE_LIST_F32(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return false;
-  }
-}
-template <>
-cudaError_t Launch<float>::plane(const PassGeom& gx, const PassGeom& gy, const C* src, C* mid, C* dst,
-                               const PassTables<C>& tb, int planes, int cluster, cudaStream_t s) {
-  switch (gx.L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT)                                                            \
-  case L_:                                                                                       \
-    return launch_cluster(k_fft_plane<float, L_, A, B, C_, NT>, planes, cluster, NT, L_ * 128, s,  \
-                          gx, gy, src, mid, dst, tb);
-    SHAFFT_PLANE_LIST_F32(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return cudaErrorNotSupported;
-  }
-}
-#endif
-
-#ifdef SHAFFT_INSTANTIATE_F64
-template <>
-bool Launch<double>::plane_supported(int L) {
-  switch (L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT) case L_: return true;
-    SHAFFT_PLANE_LIST_F64(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return false;
-  }
-}
-template <>
-cudaError_t Launch<double>::plane(const PassGeom& gx, const PassGeom& gy, const C* src, C* mid, C* dst,
-                               const PassTables<C>& tb, int planes, int cluster, cudaStream_t s) {
-  switch (gx.L) {
-#define SHAFFT_CASE(L_, A, B, C_, NT)                                                            \
-  case L_:                                                                                       \
-    return launch_cluster(k_fft_plane<double, L_, A, B, C_, NT>, planes, cluster, NT, L_ * 128, s,  \
-                          gx, gy, src, mid, dst, tb);
-    SHAFFT_PLANE_LIST_F64(SHAFFT_CASE)
-#undef SHAFFT_CASE
-    default: return cudaErrorNotSupported;
-  }
-}
-#endif
 
 template <typename T>
 cudaError_t Launch<T>::pass(const PassGeom& g, const C* in, C* out, const PassTables<C>& tb,

@@ -98,8 +98,9 @@ struct Step {
   // ST_PLANE: g = X phase (src -> mid), g2 = Y phase (mid -> out)
   PassGeom g2{};
   int mid_buf = BUF_DST;
-  int cluster = 8;
+  int lag = 4;
   int64_t planes = 0;
+  size_t off_ctl = 0;  // control words (4 + planes ints) in the plan's table blob
 };
 
 struct LTable {
@@ -160,10 +161,8 @@ struct Planner {
   int64_t scratch_elems = 0;
 
   explicit Planner(int prec) : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {
-    if (const char* e = getenv("SHAFFT_SM100_PLANE_CLUSTER")) {
-      const int v = atoi(e);
-      plane_cluster = (v == 0) ? -1 : v;  // 0 disables the fused plane pass
-    }
+    if (const char* e = getenv("SHAFFT_SM100_PLANE")) plane_enabled = atoi(e) != 0;
+    if (const char* e = getenv("SHAFFT_SM100_FLOW_LAG")) flow_lag = std::max(1, atoi(e));
   }
 
   // specialised-pass eligibility: length, tile width and 16-byte alignment
@@ -304,7 +303,7 @@ struct Planner {
   // The last two axes of a stack of O square L x L planes in one HBM pass
   // (k_fft_plane): buf -> (mid = other(buf)) -> buf.
   bool plane_step(std::vector<Step>& out, int64_t O, int64_t L, int buf) {
-    if (plane_cluster < 1 || plane_cluster > 8 || !plane_len(L) || L % fast_w() || O < 16) return false;
+    if (!plane_enabled || !plane_len(L) || L % fast_w() || O < 16 || O > (1 << 24)) return false;
     std::vector<Step> tmp;
     if (!transposed_pair(tmp, O, L, L, buf, other_buf(buf), buf)) return false;
     Step st;
@@ -317,11 +316,13 @@ struct Planner {
     st.tabL = tmp[0].tabL;
     st.smem = (size_t)L * 128;
     st.planes = O;
-    st.cluster = plane_cluster;
+    st.lag = flow_lag;
+    st.off_ctl = alloc(sizeof(int) * (size_t)(4 + O));
     out.push_back(st);
     return true;
   }
-  int plane_cluster = -1;  // fused plane pass off unless SHAFFT_SM100_PLANE_CLUSTER selects a cluster size
+  int plane_enabled = 0;  // SHAFFT_SM100_PLANE=1 turns the fused plane pass on (slower so far)
+  int flow_lag = 4;       // SHAFFT_SM100_FLOW_LAG: planes between an X tile and its Y tile
 
   // The last two axes (A = rows, Lr = contiguous) as two transposing passes:
   // rows of Lr -> [o][kL][a] in `mid`, then rows of A -> [o][ka][kL] in
@@ -752,8 +753,9 @@ struct Launcher {
     gy.conj_in = 0;
     gy.conj_out = conj_out;
     gy.scale = scale;
+    int* ctl = reinterpret_cast<int*>(p->d_tables + st.off_ctl);
     return check(K::plane(gx, gy, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(mid),
-                          reinterpret_cast<C*>(out), tables(p, st), (int)st.planes, st.cluster, s),
+                          reinterpret_cast<C*>(out), tables(p, st), (int)st.planes, ctl, st.lag, s),
                  "plane pass");
   }
 
@@ -850,8 +852,8 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
     char b[768];
     if (st.kind == ST_PLANE) {
       snprintf(b, sizeof(b),
-               "{\"kind\":\"plane\",\"L\":%d,\"planes\":%lld,\"cluster\":%d,\"in\":\"%s\",\"mid\":\"%s\",\"out\":\"%s\",\"fast\":1}",
-               st.g.L, (long long)st.planes, st.cluster, buf_name(st.in_buf), buf_name(st.mid_buf),
+               "{\"kind\":\"plane\",\"L\":%d,\"planes\":%lld,\"lag\":%d,\"in\":\"%s\",\"mid\":\"%s\",\"out\":\"%s\",\"fast\":1}",
+               st.g.L, (long long)st.planes, st.lag, buf_name(st.in_buf), buf_name(st.mid_buf),
                buf_name(st.out_buf));
     } else if (st.kind == ST_PASS) {
       std::string rad;
@@ -1041,6 +1043,20 @@ int shafft_sm100_scale(void* data, size_t count, int precision, double factor, v
     e = Launch<float>::scale_copy(reinterpret_cast<const float2*>(data),
                                   reinterpret_cast<float2*>(data), n, (float)factor, 0, s);
   CUDA_TRY(e);
+  return 0;
+}
+
+int shafft_sm100_plan_status(shafft_sm100_plan plan) {
+  if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
+  for (const Step& st : plan->steps) {
+    if (st.kind != ST_PLANE) continue;
+    int flag = 0;
+    CUDA_TRY(cudaMemcpy(&flag, plan->d_tables + st.off_ctl + 2 * sizeof(int), sizeof(int),
+                        cudaMemcpyDeviceToHost));
+    if (flag)
+      return set_err(SHAFFT_SM100_ECUDA,
+                     "fused plane pass: a wait for a plane's first-axis tiles timed out");
+  }
   return 0;
 }
 

@@ -147,11 +147,13 @@ def test_error_state_is_thread_local():
 
 def test_planner_pass_lists():
     """Host-only planner: pass structure of the headline and config shapes."""
+    # headline: transposing X and Y passes, then the Z column pass
     q = _sm100.plan_query([512, 512, 512], 0)
-    assert [s["kind"] for s in q["steps"]] == ["pass"] * len(q["steps"])
-    assert len(q["steps"]) <= 3
+    assert [s["kind"] for s in q["steps"]] == ["pass"] * 3
+    assert [s["in_row"] for s in q["steps"]] == [1, 1, 0]
+    assert all(s["fast"] for s in q["steps"])
     q = _sm100.plan_query([256, 256, 256], 1)
-    assert len(q["steps"]) <= 3
+    assert [s["kind"] for s in q["steps"]] == ["pass"] * 3
     q = _sm100.plan_query([1000003], 0)
     kinds = [s["kind"] for s in q["steps"]]
     assert kinds[0] == "bluestein_modulate" and kinds[-1] == "bluestein_demodulate"
