@@ -108,6 +108,30 @@ int64_t shafft_sm100_step_bytes(shafft_sm100_plan plan, int step);
 /* JSON description of a created plan. */
 int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen);
 
+/* ---- Batched form: many independent transforms in one launch ----------
+ * (no counterpart in the reference, which runs one plan per transform).
+ *
+ * count transforms; transform i has ndims[i] axes whose lengths follow in
+ * `dims` (flattened, row-major, last axis fastest).  Every axis length must
+ * factor into 2,3,5,7,11,13 and be <= 4096, or be <= 256 (direct DFT).
+ * flags bit 0: autotune tile widths for lengths not yet in the tuning cache
+ * (file SHAFFT_SM100_TUNE_CACHE, default ~/.cache/shafft_sm100_tune.txt).
+ * execute: src[i] -> dst[i] for every i (device pointers; src[i] is only
+ * read; src[i] == dst[i] is allowed), all transforms in one persistent kernel
+ * launch replayed from a CUDA graph captured on the first call with that
+ * direction and scale.  Asynchronous on `stream`. */
+typedef struct shafft_sm100_batch_s* shafft_sm100_batch;
+int shafft_sm100_batch_create(shafft_sm100_batch* out, int count, const int* ndims,
+                              const int64_t* dims, int precision, int flags);
+int shafft_sm100_batch_execute(shafft_sm100_batch b, void* const* src, void* const* dst,
+                               int direction, double scale, void* stream);
+int shafft_sm100_batch_destroy(shafft_sm100_batch b);
+/* error flag of the last executes (call after synchronising) */
+int shafft_sm100_batch_status(shafft_sm100_batch b);
+/* algorithmic HBM bytes of one execute (read + write per pass) */
+int64_t shafft_sm100_batch_bytes(shafft_sm100_batch b);
+int shafft_sm100_batch_describe(shafft_sm100_batch b, char* buf, int buflen);
+
 /* Device memory and stream helpers, so that callers above this ABI need no
  * CUDA runtime of their own (they replace the reference's allocBufferT /
  * freeBufferT / copyToBufferT / copyFromBufferT,

@@ -51,6 +51,17 @@ def load():
     lib.shafft_sm100_execute_step.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_double, vp]
     lib.shafft_sm100_step_bytes.argtypes = [vp, ctypes.c_int]
     lib.shafft_sm100_step_bytes.restype = ctypes.c_int64
+    lib.shafft_sm100_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int), i64p, ctypes.c_int,
+                                              ctypes.c_int]
+    lib.shafft_sm100_batch_execute.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                               ctypes.c_int, ctypes.c_double, vp]
+    lib.shafft_sm100_batch_destroy.argtypes = [vp]
+    lib.shafft_sm100_batch_status.argtypes = [vp]
+    lib.shafft_sm100_batch_bytes.argtypes = [vp]
+    lib.shafft_sm100_batch_bytes.restype = ctypes.c_int64
+    lib.shafft_sm100_batch_describe.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    lib.shafft_sm100_plan_status.argtypes = [vp]
     lib.shafft_sm100_last_error_message.restype = ctypes.c_char_p
     lib.shafft_sm100_version.restype = ctypes.c_char_p
     _lib = lib
@@ -130,3 +141,51 @@ class Plan:
 def scale(ptr: int, count: int, precision: int, factor: float, stream: int = 0):
     _check(load().shafft_sm100_scale(ctypes.c_void_p(ptr), count, precision, factor,
                                      ctypes.c_void_p(stream)), "scale")
+
+
+class Batch:
+    """Many independent transforms of different shapes, one launch per execute
+    (shafft_sm100_batch_*)."""
+
+    def __init__(self, shapes, precision=0, autotune=False):
+        lib = load()
+        self._lib = lib
+        self.shapes = [tuple(int(d) for d in s) for s in shapes]
+        self.precision = int(precision)
+        nd = (ctypes.c_int * len(self.shapes))(*[len(s) for s in self.shapes])
+        flat = [d for s in self.shapes for d in s]
+        dims = (ctypes.c_int64 * len(flat))(*flat)
+        h = ctypes.c_void_p()
+        _check(lib.shafft_sm100_batch_create(ctypes.byref(h), len(self.shapes), nd, dims,
+                                             self.precision, 1 if autotune else 0), "batch_create")
+        self.handle = h
+
+    def execute(self, src_ptrs, dst_ptrs, direction=0, scale=1.0, stream=0):
+        n = len(self.shapes)
+        s = (ctypes.c_void_p * n)(*src_ptrs)
+        d = (ctypes.c_void_p * n)(*dst_ptrs)
+        _check(self._lib.shafft_sm100_batch_execute(self.handle, s, d, int(direction), float(scale),
+                                                    ctypes.c_void_p(stream)), "batch_execute")
+
+    def status(self):
+        _check(self._lib.shafft_sm100_batch_status(self.handle), "batch_status")
+
+    @property
+    def alg_bytes(self) -> int:
+        return int(self._lib.shafft_sm100_batch_bytes(self.handle))
+
+    def describe(self) -> dict:
+        buf = ctypes.create_string_buffer(4096)
+        _check(self._lib.shafft_sm100_batch_describe(self.handle, buf, len(buf)), "describe")
+        return json.loads(buf.value.decode())
+
+    def destroy(self):
+        if self.handle:
+            self._lib.shafft_sm100_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -116,13 +116,56 @@ __host__ __device__ constexpr int ilog2c(int x) {
   return l;
 }
 
+// Direct DFT of the tile held in shared memory (natural order, [n][w] with
+// the given pitch): X[k] = sum_n x[n] w_L^{nk}, the exponent n*k reduced
+// modulo L incrementally.  Used for lengths with a prime factor above 13 when
+// L is small enough that O(L) work per output beats a Bluestein round trip.
+// Outputs go straight to HBM with the pass's fused twiddle/scale/conj.
+template <typename T, typename C>
+__device__ __forceinline__ void direct_store(const PassGeom& g, const PassTables<C>& tb, const C* sm,
+                                             C* out, int L, int W, int logW, int pitch, int wcount,
+                                             int64_t bout, int64_t w0, int64_t tconst) {
+  const int total = L << logW;
+  const T scale = (T)g.scale;
+  for (int b = threadIdx.x; b < total; b += kThreads) {
+    int w, k;
+    if (g.out_row) {
+      k = b % L;
+      w = b / L;
+    } else {
+      w = b & (W - 1);
+      k = b >> logW;
+    }
+    if (w >= wcount) continue;
+    T ar = 0, ai = 0;
+    int m = 0;
+    for (int n = 0; n < L; ++n) {
+      const C x = sm[n * pitch + w];
+      const C t = tb.twL[m];
+      ar += x.x * t.x - x.y * t.y;
+      ai += x.x * t.y + x.y * t.x;
+      m += k;
+      if (m >= L) m -= L;
+    }
+    C y = C{ar, ai};
+    if (g.tw_mode == TW_POST) {
+      const int64_t tt = (g.tw_dim == 0) ? (w0 + w) : tconst;
+      y = cmul(y, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * tt));
+    }
+    if (g.scale != 1.0) y = cscale(y, scale);
+    if (g.conj_out) y.y = -y.y;
+    out[bout + (int64_t)w * g.sout[0] + (int64_t)k * g.sk_out] = y;
+  }
+}
+
+// One W-wide tile of a generic pass (runtime length and radix list; nst == 0
+// selects the direct DFT).  `sm` holds L * pitch elements.
 template <typename T, int LS, int WS>
-__global__ void __launch_bounds__(kThreads)
-    k_fft_pass(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
-               typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+__device__ __forceinline__ void generic_tile(const PassGeom& g, const typename Cx<T>::type* in,
+                                             typename Cx<T>::type* out,
+                                             const PassTables<typename Cx<T>::type>& tb, int64_t tile,
+                                             typename Cx<T>::type* sm) {
   using C = typename Cx<T>::type;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  C* sm = reinterpret_cast<C*>(smem_raw);
   constexpr RadixPlan P = radix_plan(LS > 0 ? LS : 1);
   const int L = LS ? LS : g.L;
   const int W = WS ? WS : g.W;
@@ -130,70 +173,105 @@ __global__ void __launch_bounds__(kThreads)
   const int pitch = WS ? (WS == 1 ? 1 : WS + 1) : g.pitch;
   const int nst = LS ? P.n : g.nst;
 
-  for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
-    int64_t rest = tile;
-    const int64_t tw = rest % g.tiles_w;
-    rest /= g.tiles_w;
-    const int64_t i1 = rest % g.ext[1];
-    rest /= g.ext[1];
-    const int64_t i2 = rest % g.ext[2];
-    const int64_t i3 = rest / g.ext[2];
-    const int64_t w0 = tw * W;
-    const int wcount = (int)((g.ext[0] - w0) < W ? (g.ext[0] - w0) : W);
-    const int64_t bin = w0 * g.sin[0] + i1 * g.sin[1] + i2 * g.sin[2] + i3 * g.sin[3];
-    const int64_t bout = w0 * g.sout[0] + i1 * g.sout[1] + i2 * g.sout[2] + i3 * g.sout[3];
-    const int64_t tconst = g.tw_dim == 1 ? i1 : (g.tw_dim == 2 ? i2 : (g.tw_dim == 3 ? i3 : 0));
+  int64_t rest = tile;
+  const int64_t tw = rest % g.tiles_w;
+  rest /= g.tiles_w;
+  const int64_t i1 = rest % g.ext[1];
+  rest /= g.ext[1];
+  const int64_t i2 = rest % g.ext[2];
+  const int64_t i3 = rest / g.ext[2];
+  const int64_t w0 = tw * W;
+  const int wcount = (int)((g.ext[0] - w0) < W ? (g.ext[0] - w0) : W);
+  const int64_t bin = w0 * g.sin[0] + i1 * g.sin[1] + i2 * g.sin[2] + i3 * g.sin[3];
+  const int64_t bout = w0 * g.sout[0] + i1 * g.sout[1] + i2 * g.sout[2] + i3 * g.sout[3];
+  const int64_t tconst = g.tw_dim == 1 ? i1 : (g.tw_dim == 2 ? i2 : (g.tw_dim == 3 ? i3 : 0));
 
-    // phase 1: load + first radix stage
-    {
-      const int r0 = LS ? P.r[0] : g.rad[0];
-#define SHAFFT_CALL_FIRST(R) \
-  stage_first<R, C>(g, tb, in, sm, L, W, logW, pitch, nst, wcount, bin, w0, tconst)
-      SHAFFT_RADIX_DISPATCH(r0, SHAFFT_CALL_FIRST)
-#undef SHAFFT_CALL_FIRST
+  if (!LS && nst == 0) {
+    // direct DFT: load the tile in natural order, then O(L) per output
+    const int total = L << logW;
+    for (int b = threadIdx.x; b < total; b += kThreads) {
+      int w, n;
+      if (g.in_row) {
+        n = b % L;
+        w = b / L;
+      } else {
+        w = b & (W - 1);
+        n = b >> logW;
+      }
+      C x = (w < wcount) ? in[bin + (int64_t)w * g.sin[0] + (int64_t)n * g.sn_in] : C{0, 0};
+      if (g.conj_in) x.y = -x.y;
+      if (g.tw_mode == TW_PRE) {
+        const int64_t t = (g.tw_dim == 0) ? (w0 + w) : tconst;
+        x = cmul(x, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)n * t));
+      }
+      sm[n * pitch + w] = x;
     }
     __syncthreads();
-    // phase 2: remaining stages in shared memory
-    {
-      int span = L;
+    direct_store<T, C>(g, tb, sm, out, L, W, logW, pitch, wcount, bout, w0, tconst);
+    return;
+  }
+
+  // phase 1: load + first radix stage
+  {
+    const int r0 = LS ? P.r[0] : g.rad[0];
+#define SHAFFT_CALL_FIRST(R) \
+  stage_first<R, C>(g, tb, in, sm, L, W, logW, pitch, nst, wcount, bin, w0, tconst)
+    SHAFFT_RADIX_DISPATCH(r0, SHAFFT_CALL_FIRST)
+#undef SHAFFT_CALL_FIRST
+  }
+  __syncthreads();
+  // phase 2: remaining stages in shared memory
+  {
+    int span = L;
 #pragma unroll
-      for (int s = 1; s < (LS ? P.n : kMaxStages); ++s) {
-        if (!LS && s >= nst) break;
-        span /= (LS ? P.r[s - 1] : g.rad[s - 1]);
-        const int Ls = L / span;
-        const int rs = LS ? P.r[s] : g.rad[s];
+    for (int s = 1; s < (LS ? P.n : kMaxStages); ++s) {
+      if (!LS && s >= nst) break;
+      span /= (LS ? P.r[s - 1] : g.rad[s - 1]);
+      const int Ls = L / span;
+      const int rs = LS ? P.r[s] : g.rad[s];
 #define SHAFFT_CALL_MID(R) stage_mid<R, C>(tb, sm, L, W, logW, pitch, span, Ls)
-        SHAFFT_RADIX_DISPATCH(rs, SHAFFT_CALL_MID)
+      SHAFFT_RADIX_DISPATCH(rs, SHAFFT_CALL_MID)
 #undef SHAFFT_CALL_MID
-        __syncthreads();
-      }
+      __syncthreads();
     }
-    // phase 3: digit-reversed read, fused twiddle/scale/conj, store
-    {
-      const int total = L << logW;
-      const T scale = (T)g.scale;
-      for (int b = threadIdx.x; b < total; b += kThreads) {
-        int w, p, k;
-        if (g.out_row) {
-          k = b % L;
-          w = b / L;
-          p = tb.k2p[k];
-        } else {
-          w = b & (W - 1);
-          p = b >> logW;
-          k = tb.p2k[p];
-        }
-        if (w >= wcount) continue;
-        C x = sm[p * pitch + w];
-        if (g.tw_mode == TW_POST) {
-          const int64_t t = (g.tw_dim == 0) ? (w0 + w) : tconst;
-          x = cmul(x, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * t));
-        }
-        if (g.scale != 1.0) x = cscale(x, scale);
-        if (g.conj_out) x.y = -x.y;
-        out[bout + (int64_t)w * g.sout[0] + (int64_t)k * g.sk_out] = x;
+  }
+  // phase 3: digit-reversed read, fused twiddle/scale/conj, store
+  {
+    const int total = L << logW;
+    const T scale = (T)g.scale;
+    for (int b = threadIdx.x; b < total; b += kThreads) {
+      int w, p, k;
+      if (g.out_row) {
+        k = b % L;
+        w = b / L;
+        p = tb.k2p[k];
+      } else {
+        w = b & (W - 1);
+        p = b >> logW;
+        k = tb.p2k[p];
       }
+      if (w >= wcount) continue;
+      C x = sm[p * pitch + w];
+      if (g.tw_mode == TW_POST) {
+        const int64_t t = (g.tw_dim == 0) ? (w0 + w) : tconst;
+        x = cmul(x, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * t));
+      }
+      if (g.scale != 1.0) x = cscale(x, scale);
+      if (g.conj_out) x.y = -x.y;
+      out[bout + (int64_t)w * g.sout[0] + (int64_t)k * g.sk_out] = x;
     }
+  }
+}
+
+template <typename T, int LS, int WS>
+__global__ void __launch_bounds__(kThreads)
+    k_fft_pass(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
+               typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
+  using C = typename Cx<T>::type;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  for (int64_t tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+    generic_tile<T, LS, WS>(g, in, out, tb, tile, sm);
     __syncthreads();
   }
 }

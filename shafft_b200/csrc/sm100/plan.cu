@@ -132,6 +132,9 @@ static Limits limits_for(int precision) {
   return Limits{4096, 2048, 4096, 8};
 }
 
+// longest non-smooth length handled by a direct-DFT pass
+constexpr int64_t kDirectMax = 128;
+
 static bool is_smooth(int64_t L) {
   const int64_t primes[] = {2, 3, 5, 7, 11, 13};
   for (int64_t p : primes)
@@ -232,11 +235,13 @@ struct Planner {
     return (int)ntabs.size() - 1;
   }
 
+  // radix stages of a pass of length L; nst = 0 (direct DFT) when L has a
+  // prime factor above 13
   void fill_radix(PassGeom& g, int L) {
     RadixPlan rp = radix_plan(L);
     g.L = L;
-    g.nst = rp.n;
-    for (int s = 0; s < rp.n; ++s) g.rad[s] = rp.r[s];
+    g.nst = rp.n > 0 ? rp.n : 0;
+    for (int s = 0; s < g.nst; ++s) g.rad[s] = rp.r[s];
   }
 
   void finish_geom(Step& st, int W) {
@@ -519,6 +524,14 @@ struct Planner {
       }
     }
     if (in_bluestein) return SHAFFT_SM100_ENOTSUP;
+    // short lengths with a large prime factor: one direct-DFT pass (O(L)
+    // work per output) instead of the five Bluestein steps
+    if (L <= kDirectMax) {
+      int ob = force_oop ? other_buf(cur) : cur;
+      single_pass(out, O, (int)L, I, cur, ob);
+      cur = ob;
+      return 0;
+    }
     // Bluestein
     int64_t M = 1;
     while (M < 2 * L - 1) M <<= 1;
