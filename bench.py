@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--dims", default=None, help="override the 512^3 workload (debug only)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--suite", default="headline", choices=["headline", "batched", "serve", "configs"],
+                    help="headline (default, the contract line) or one of the side workloads")
+    ap.add_argument("--count", type=int, default=4096, help="transforms of the batched suite")
     return ap.parse_args()
 
 
@@ -392,10 +395,292 @@ def e2e_arm(S, dims, n, args, stream, barrier, dist):
                     "shafftCopyFromBufferF, pinned host buffers"}
 
 
+# ---------------------------------------------------------------------------
+# side workloads (not the contract line)
+# ---------------------------------------------------------------------------
+
+def _is_smooth7(n):
+    for p in (2, 3, 5, 7):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
+def _is_prime(n):
+    return n > 1 and all(n % d for d in range(2, int(n ** 0.5) + 1))
+
+
+def batched_shapes(count=4096, seed=42):
+    """Seeded uneven 2-D/3-D shapes: extents log-uniform in [16, 256] over the
+    7-smooth numbers, 5% drawn from the primes in [16, 256]."""
+    import numpy as np
+    rng = np.random.Generator(np.random.MT19937(seed))
+    smooth = [n for n in range(16, 257) if _is_smooth7(n)]
+    lsm = np.log(np.array(smooth, dtype=np.float64))
+    primes = [p for p in range(16, 257) if _is_prime(p)]
+    shapes = []
+    for _ in range(count):
+        nd = 2 if rng.uniform() < 0.5 else 3
+        dims = []
+        for _ in range(nd):
+            if rng.uniform() < 0.05:
+                dims.append(int(primes[int(rng.integers(0, len(primes)))]))
+            else:
+                v = rng.uniform(np.log(16), np.log(256))
+                dims.append(int(smooth[int(np.argmin(np.abs(lsm - v)))]))
+        shapes.append(tuple(dims))
+    return shapes
+
+
+def suite_batched(args):
+    import numpy as np
+    import torch
+
+    import shafft_b200 as S  # noqa: F401
+    from oracle import oracle as o
+    from shafft_b200 import _sm100
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    shapes = batched_shapes(args.count)
+    sizes = [math.prod(s) for s in shapes]
+    offs, tot = [], 0
+    for n in sizes:
+        offs.append(tot)
+        tot += (n + 63) // 64 * 64
+    gen = torch.Generator(device="cuda").manual_seed(42)
+    src = (torch.rand(2 * tot, device="cuda", generator=gen) * 2 - 1).view(torch.complex64)
+    dst = torch.empty_like(src)
+    scr = torch.empty_like(src)
+    sp = [src.data_ptr() + 8 * off for off in offs]
+    dp = [dst.data_ptr() + 8 * off for off in offs]
+    cp = [scr.data_ptr() + 8 * off for off in offs]
+    stream = torch.cuda.current_stream()
+    t0 = time.perf_counter()
+    batch = _sm100.Batch(shapes, 0, autotune=True)
+    t_create = time.perf_counter() - t0
+    for _ in range(2):
+        batch.execute(sp, dp, 0, 1.0, stream.cuda_stream)
+    torch.cuda.synchronize()
+    k = max(3, min(args.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        batch.execute(sp, dp, 0, 1.0, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batch.status()
+    t_batch = e0.elapsed_time(e1) / k
+    # sampled parity against the oracle
+    rng = np.random.Generator(np.random.MT19937(7))
+    small = [i for i, n in enumerate(sizes) if n <= (1 << 20)]
+    sample = sorted(set(rng.choice(small, size=min(24, len(small)), replace=False).tolist()
+                        + [i for i in small if any(_is_prime(d) for d in shapes[i])][:8]))
+    errs = []
+    for i in sample:
+        x = src[offs[i]:offs[i] + sizes[i]].cpu().numpy().reshape(shapes[i])
+        y = dst[offs[i]:offs[i] + sizes[i]].cpu().numpy().reshape(shapes[i])
+        errs.append(o.rel_l2(y, o.fftn(x.astype(np.complex128))))
+    # the plain path: one plan per transform, launched one by one
+    t0 = time.perf_counter()
+    plans = {}
+    for s in shapes:
+        if s not in plans:
+            plans[s] = _sm100.Plan(s, 0)
+    t_plans = time.perf_counter() - t0
+    launches = sum(plans[s].launches for s in shapes)
+
+    def plain():
+        for i, s in enumerate(shapes):
+            plans[s].execute(cp[i], dp[i], 0, 1.0, stream.cuda_stream)
+    scr.copy_(src)
+    plain()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(2):
+        plain()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_plain = e0.elapsed_time(e1) / 2
+    comp = sum(2 * 8 * n for n in sizes)
+    out = {
+        "metric": "batched uneven 2-D/3-D c64 forward transforms: compulsory GB/s", "unit": "GB/s",
+        "value": comp / (t_batch / 1e3) / 1e9, "plain_value": comp / (t_plain / 1e3) / 1e9,
+        "speedup_vs_plain": t_plain / t_batch, "ms_batched": t_batch, "ms_plain": t_plain,
+        "transforms": len(shapes), "elements": sum(sizes),
+        "plan_hbm_gbs_batched": batch.alg_bytes / (t_batch / 1e3) / 1e9,
+        "launches_batched_per_execute": 1, "launches_plain_per_execute": launches,
+        "create_s": {"batch_with_autotune": t_create, "plain_plans": t_plans},
+        "batch": batch.describe(), "max_rel_l2_sample": max(errs), "sample": len(errs),
+        "tol_c64": "1e-6*log2(N)", "data": "synthetic",
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+SERVE_1D = [1 << e for e in range(10, 23)]
+SERVE_2D = [64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048]
+SERVE_3D = [32, 48, 64, 96, 128, 192, 256, 384]
+SERVE_PRIMES = {1: [1031, 16411, 262147, 1048583], 2: [97, 211, 509, 1021], 3: [37, 97, 131, 257]}
+
+
+def serve_requests(count, seed=42):
+    """Seeded request mix: equal shares of 1-D (2^10..2^22), 2-D (64^2..2048^2)
+    and 3-D (32^3..384^3) sizes drawn log-uniformly from a fixed ladder (so
+    shapes repeat and plans stay resident), 30% complex128, 10% with a prime
+    length, forward/backward 50/50."""
+    import numpy as np
+    rng = np.random.Generator(np.random.MT19937(seed))
+    out = []
+    for _ in range(count):
+        cls = int(rng.integers(1, 4))
+        ladder = {1: SERVE_1D, 2: SERVE_2D, 3: SERVE_3D}[cls]
+        n = ladder[int(rng.integers(0, len(ladder)))]
+        dims = [n] * cls
+        if rng.uniform() < 0.10:
+            dims[int(rng.integers(0, cls))] = int(rng.choice(SERVE_PRIMES[cls]))
+        prec = 1 if rng.uniform() < 0.30 else 0
+        out.append((tuple(dims), prec, int(rng.integers(0, 2))))
+    return out
+
+
+def suite_serve(args):
+    import numpy as np
+    import torch
+
+    from shafft_b200 import _sm100
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    reqs = serve_requests(max(40, min(args.count, 400)))
+    maxb = max(math.prod(d) * (16 if p else 8) for d, p, _ in reqs)
+    hin = torch.empty(maxb // 4, dtype=torch.float32, pin_memory=True).uniform_(-1, 1)
+    hout = torch.empty(maxb // 4, dtype=torch.float32, pin_memory=True)
+    # serial baseline: one request at a time through a resident plan
+    plans = {}
+    dev = torch.empty(maxb // 4, dtype=torch.float32, device="cuda")
+    dev2 = torch.empty_like(dev)
+    lib = _sm100.load()
+
+    def serial_one(dims, prec, direction):
+        key = (dims, prec)
+        if key not in plans:
+            plans[key] = _sm100.Plan(dims, prec)
+        nb = math.prod(dims) * (16 if prec else 8)
+        t0 = time.perf_counter()
+        lib.shafft_sm100_memcpy(ctypes.c_void_p(dev.data_ptr()), ctypes.c_void_p(hin.data_ptr()), nb, 1, None)
+        plans[key].execute(dev.data_ptr(), dev2.data_ptr(), direction, 1.0, 0)
+        lib.shafft_sm100_memcpy(ctypes.c_void_p(hout.data_ptr()), ctypes.c_void_p(dev2.data_ptr()), nb, 2, None)
+        return (time.perf_counter() - t0) * 1e3
+    for d, p, r in reqs:  # warm plans
+        serial_one(d, p, r)
+    t0 = time.perf_counter()
+    lat = [serial_one(d, p, r) for d, p, r in reqs]
+    serial_s = time.perf_counter() - t0
+    serial_tput = len(reqs) / serial_s
+    lat.sort()
+    serial = {"throughput_per_s": serial_tput, "p50_ms": lat[len(lat) // 2],
+              "p99_ms": lat[min(len(lat) - 1, int(0.99 * (len(lat) - 1) + 0.5))]}
+    del plans, dev, dev2
+    torch.cuda.empty_cache()
+    srv = _sm100.Server(budget_bytes=40 << 30, streams=8)
+    # warm the server's plan cache with one pass over the mix
+    ids = [srv.submit(d, p, r, 1.0, hin.data_ptr(), hout.data_ptr()) for d, p, r in reqs]
+    for i in ids:
+        srv.wait(i)
+    rng = np.random.Generator(np.random.MT19937(5))
+    sweep = []
+    for mult in (0.5, 1.0, 2.0, 4.0, 8.0):
+        rate = mult * serial_tput
+        gaps = rng.exponential(1.0 / rate, size=len(reqs))
+        srv.reset_stats()
+        start = time.perf_counter()
+        due = start
+        ids = []
+        for (d, p, r), gap in zip(reqs, gaps):
+            due += gap
+            now = time.perf_counter()
+            if due > now:
+                time.sleep(due - now)
+            ids.append(srv.submit(d, p, r, 1.0, hin.data_ptr(), hout.data_ptr()))
+        for i in ids:
+            srv.wait(i)
+        wall = time.perf_counter() - start
+        st = srv.stats()
+        st["offered_per_s"] = rate
+        st["achieved_per_s"] = len(reqs) / wall
+        sweep.append(st)
+    srv.destroy()
+    best = max(s["achieved_per_s"] for s in sweep)
+    out = {"metric": "served mixed C2C requests: throughput and p50/p99 latency", "unit": "requests/s",
+           "value": best, "serial_plain": serial, "speedup_vs_serial": best / serial_tput,
+           "requests": len(reqs), "budget_bytes": 40 << 30, "streams": 8, "sweep": sweep,
+           "host_buffers": "pinned, shared by all requests (timing only)", "data": "synthetic"}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def suite_configs(args):
+    import numpy as np
+    import torch
+
+    from oracle import oracle as o
+    from shafft_b200 import _sm100
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.current_stream()
+    peak, _ = peaks()
+    res = []
+
+    def run(dims, prec, reps, check):
+        n = math.prod(dims)
+        dt = torch.complex128 if prec else torch.complex64
+        es = 16 if prec else 8
+        x = o.uniform_input(dims, seed=42, dtype=np.complex128 if prec else np.complex64) if check else None
+        a = torch.from_numpy(x.ravel()).cuda() if check else torch.randn(n, dtype=dt, device="cuda")
+        a0 = a.clone()
+        b = torch.empty_like(a)
+        p = _sm100.Plan(dims, prec)
+        err = None
+        if check:
+            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+            y = b.cpu().numpy()
+            err = o.rel_l2(y, o.fftn(x.astype(np.complex128), precise=bool(prec)).ravel())
+        for _ in range(3):
+            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+            p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+            p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        comp = 2 * 2 * es * n
+        res.append({"dims": list(dims), "precision": "c128" if prec else "c64", "ms_fwd_bwd": ms,
+                    "compulsory_gbs": comp / (ms / 1e3) / 1e9,
+                    "plan_gbs": 2 * sum(p.step_bytes(i) for i in range(p.launches)) / (ms / 1e3) / 1e9,
+                    "pct_hbm_plan": 100 * 2 * sum(p.step_bytes(i) for i in range(p.launches)) / (ms / 1e3) / 1e9 / peak,
+                    "launches_per_transform": p.launches,
+                    "rel_l2_vs_oracle": err,
+                    "tol": (1e-6 if prec == 0 else 1e-14) * math.log2(n)})
+        del a, a0, b
+        p.destroy()
+    run((256, 256, 256), 1, 20, False)
+    run((64, 64, 32), 0, 50, True)
+    for n in (1 << 24, 1488375, 1000003):
+        for prec in (0, 1):
+            run((n,), prec, 10, True)
+    print(json.dumps({"metric": "BASELINE configs: fwd+bwd time and error", "configs": res}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.suite == "batched":
+        return suite_batched(args)
+    if args.suite == "serve":
+        return suite_serve(args)
+    if args.suite == "configs":
+        return suite_configs(args)
     return ours(args)
 
 

@@ -132,6 +132,27 @@ int shafft_sm100_batch_status(shafft_sm100_batch b);
 int64_t shafft_sm100_batch_bytes(shafft_sm100_batch b);
 int shafft_sm100_batch_describe(shafft_sm100_batch b, char* buf, int buflen);
 
+/* ---- Serving form: request loop with continuous admission ---------------
+ * (no counterpart in the reference).  A server owns `streams` CUDA streams,
+ * a dispatcher thread and a completion thread.  Requests (host input/output
+ * buffers -- pinned for overlap) are admitted in arrival order as soon as
+ * their two device buffers fit `budget_bytes` (resident plans count against
+ * the budget; idle plans are evicted oldest first), issued on the least
+ * recently used stream (H2D, execute, D2H) and so overlap with requests
+ * already running.  wait() blocks until the request's output is in
+ * host_out and returns its status and latency (submission to completion).
+ * stats() reports completed / failed counts, p50 / p99 / max latency and
+ * throughput as JSON.  Wait for every submitted request before destroy. */
+typedef struct shafft_sm100_server_s* shafft_sm100_server;
+int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, int streams);
+int shafft_sm100_server_submit(shafft_sm100_server s, int ndim, const int64_t* dims, int precision,
+                               int direction, double scale, const void* host_in, void* host_out,
+                               uint64_t* id);
+int shafft_sm100_server_wait(shafft_sm100_server s, uint64_t id, double* latency_ms);
+int shafft_sm100_server_stats(shafft_sm100_server s, char* buf, int buflen);
+int shafft_sm100_server_reset_stats(shafft_sm100_server s);
+int shafft_sm100_server_destroy(shafft_sm100_server s);
+
 /* Device memory and stream helpers, so that callers above this ABI need no
  * CUDA runtime of their own (they replace the reference's allocBufferT /
  * freeBufferT / copyToBufferT / copyFromBufferT,

@@ -62,6 +62,13 @@ def load():
     lib.shafft_sm100_batch_bytes.restype = ctypes.c_int64
     lib.shafft_sm100_batch_describe.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     lib.shafft_sm100_plan_status.argtypes = [vp]
+    lib.shafft_sm100_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_size_t, ctypes.c_int]
+    lib.shafft_sm100_server_submit.argtypes = [vp, ctypes.c_int, i64p, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_double, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+    lib.shafft_sm100_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)]
+    lib.shafft_sm100_server_stats.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    lib.shafft_sm100_server_reset_stats.argtypes = [vp]
+    lib.shafft_sm100_server_destroy.argtypes = [vp]
     lib.shafft_sm100_last_error_message.restype = ctypes.c_char_p
     lib.shafft_sm100_version.restype = ctypes.c_char_p
     _lib = lib
@@ -182,6 +189,53 @@ class Batch:
     def destroy(self):
         if self.handle:
             self._lib.shafft_sm100_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop with continuous admission (shafft_sm100_server_*)."""
+
+    def __init__(self, budget_bytes, streams=4):
+        lib = load()
+        self._lib = lib
+        h = ctypes.c_void_p()
+        _check(lib.shafft_sm100_server_create(ctypes.byref(h), int(budget_bytes), int(streams)),
+               "server_create")
+        self.handle = h
+
+    def submit(self, dims, precision, direction, scale, host_in_ptr, host_out_ptr) -> int:
+        d = (ctypes.c_int64 * len(dims))(*dims)
+        rid = ctypes.c_uint64()
+        _check(self._lib.shafft_sm100_server_submit(self.handle, len(dims), d, int(precision),
+                                                    int(direction), float(scale),
+                                                    ctypes.c_void_p(host_in_ptr),
+                                                    ctypes.c_void_p(host_out_ptr), ctypes.byref(rid)),
+               "server_submit")
+        return rid.value
+
+    def wait(self, rid) -> float:
+        lat = ctypes.c_double()
+        _check(self._lib.shafft_sm100_server_wait(self.handle, ctypes.c_uint64(rid), ctypes.byref(lat)),
+               "server_wait")
+        return lat.value
+
+    def stats(self) -> dict:
+        buf = ctypes.create_string_buffer(1024)
+        _check(self._lib.shafft_sm100_server_stats(self.handle, buf, len(buf)), "server_stats")
+        return json.loads(buf.value.decode())
+
+    def reset_stats(self):
+        self._lib.shafft_sm100_server_reset_stats(self.handle)
+
+    def destroy(self):
+        if self.handle:
+            self._lib.shafft_sm100_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,0 +1,406 @@
+// Serving form: a request loop with continuous admission.
+//
+// Clients submit C2C transforms (shape, precision, direction, scale, host
+// input and output buffers) from any thread.  A dispatcher thread admits
+// requests in arrival order as soon as their device memory fits the budget:
+//   * device input/output buffers come from a stream-ordered memory pool
+//     (cudaMallocAsync / cudaFreeAsync), so freeing is ordered after the work;
+//   * plans are kept resident per shape (several instances per shape when
+//     requests of one shape overlap); idle instances are evicted oldest-first
+//     when the budget needs their memory;
+//   * each admitted request is issued on the least recently used of S streams
+//     (H2D copy, execute, D2H copy, frees), so requests that arrive while
+//     others run overlap with them on the GPU.
+// A completion thread polls the per-request events, releases the budget and
+// the plan instance, stamps the completion time and wakes waiters.  Latency
+// is completion time minus submission time; statistics report p50 / p99.
+// With the same plan arithmetic a request's result is bit-identical whether
+// it ran alone or in a mix (tested).
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../../include/shafft_sm100.h"
+#include "launch.h"
+
+namespace shafft_sm100 {
+namespace {
+
+int sfail(int code, const char* fmt, ...) {
+  char msg[256];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(msg, sizeof(msg), fmt, ap);
+  va_end(ap);
+  return report_error(code, msg);
+}
+
+using Clock = std::chrono::steady_clock;
+
+struct PlanInst {
+  shafft_sm100_plan plan = nullptr;
+  bool busy = false;
+  size_t bytes = 0;
+  Clock::time_point last_used;
+};
+
+struct Request {
+  uint64_t id = 0;
+  std::vector<int64_t> dims;
+  int precision = 0, direction = 0;
+  double scale = 1.0;
+  const void* host_in = nullptr;
+  void* host_out = nullptr;
+  size_t bytes = 0;  // one buffer
+  Clock::time_point t_submit, t_done;
+  // in flight
+  void* d_in = nullptr;
+  void* d_out = nullptr;
+  cudaEvent_t ev = nullptr;
+  PlanInst* inst = nullptr;
+  int stream = -1;
+  int status = 0;
+  bool done = false;
+};
+
+}  // namespace
+}  // namespace shafft_sm100
+
+using namespace shafft_sm100;
+
+struct shafft_sm100_server_s {
+  size_t budget = 0, used = 0;
+  int nstreams = 0;
+  std::vector<cudaStream_t> streams;
+  std::vector<Clock::time_point> stream_last;
+  cudaMemPool_t pool = nullptr;
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv_queue, cv_done;
+  std::deque<std::shared_ptr<Request>> queue;
+  std::vector<std::shared_ptr<Request>> inflight;
+  std::map<uint64_t, std::shared_ptr<Request>> all;
+  std::map<std::string, std::vector<std::unique_ptr<PlanInst>>> plans;
+  size_t plan_bytes = 0;
+  std::atomic<bool> stop{false};
+  std::thread dispatcher, completer;
+  uint64_t next_id = 1;
+  std::vector<double> latencies_ms;
+  Clock::time_point t_first, t_last;
+  uint64_t completed = 0, failed = 0;
+  int max_inflight_seen = 0;
+};
+
+namespace {
+
+std::string plan_key(const Request& r) {
+  std::string k = r.precision ? "z" : "c";
+  for (int64_t d : r.dims) k += ":" + std::to_string(d);
+  return k;
+}
+
+// caller holds s->mu; returns a free plan instance for r, creating one (and
+// evicting idle instances of other shapes if the budget needs it)
+PlanInst* acquire_plan(shafft_sm100_server_s* s, const Request& r, int* rc) {
+  auto& vec = s->plans[plan_key(r)];
+  for (auto& p : vec)
+    if (!p->busy) {
+      p->busy = true;
+      p->last_used = Clock::now();
+      return p.get();
+    }
+  shafft_sm100_plan pl = nullptr;
+  *rc = shafft_sm100_plan_create_nd(&pl, (int)r.dims.size(), r.dims.data(), r.precision);
+  if (*rc) return nullptr;
+  auto inst = std::make_unique<PlanInst>();
+  inst->plan = pl;
+  inst->bytes = shafft_sm100_plan_device_bytes(pl);
+  inst->busy = true;
+  inst->last_used = Clock::now();
+  s->plan_bytes += inst->bytes;
+  s->used += inst->bytes;
+  vec.push_back(std::move(inst));
+  return vec.back().get();
+}
+
+// caller holds s->mu: drop idle plan instances, oldest first, until `need`
+// more bytes fit the budget
+void evict_idle(shafft_sm100_server_s* s, size_t need) {
+  while (s->used + need > s->budget) {
+    PlanInst* victim = nullptr;
+    std::string vkey;
+    for (auto& kv : s->plans)
+      for (auto& p : kv.second)
+        if (!p->busy && (!victim || p->last_used < victim->last_used)) {
+          victim = p.get();
+          vkey = kv.first;
+        }
+    if (!victim) return;
+    auto& vec = s->plans[vkey];
+    for (size_t i = 0; i < vec.size(); ++i)
+      if (vec[i].get() == victim) {
+        shafft_sm100_plan_destroy(victim->plan);
+        s->plan_bytes -= victim->bytes;
+        s->used -= victim->bytes;
+        vec.erase(vec.begin() + i);
+        break;
+      }
+    if (vec.empty()) s->plans.erase(vkey);
+  }
+}
+
+void dispatcher_loop(shafft_sm100_server_s* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop) {
+    if (s->queue.empty()) {
+      s->cv_queue.wait_for(lk, std::chrono::milliseconds(20));
+      continue;
+    }
+    std::shared_ptr<Request> r = s->queue.front();
+    const size_t need = 2 * r->bytes;
+    if (s->used + need > s->budget) evict_idle(s, need);
+    if (s->used + need > s->budget) {
+      if (s->inflight.empty()) {
+        // can never fit: fail it instead of blocking the queue
+        s->queue.pop_front();
+        r->status = sfail(SHAFFT_SM100_EALLOC, "request needs %zu bytes, budget %zu", need, s->budget);
+        r->done = true;
+        r->t_done = Clock::now();
+        s->failed++;
+        s->cv_done.notify_all();
+        continue;
+      }
+      // wait for completions to free budget (FIFO admission)
+      s->cv_queue.wait_for(lk, std::chrono::microseconds(200));
+      continue;
+    }
+    s->queue.pop_front();
+    int rc = 0;
+    PlanInst* inst = acquire_plan(s, *r, &rc);
+    if (!inst) {
+      r->status = rc;
+      r->done = true;
+      r->t_done = Clock::now();
+      s->failed++;
+      s->cv_done.notify_all();
+      continue;
+    }
+    s->used += need;
+    // least recently used stream
+    int si = 0;
+    for (int i = 1; i < s->nstreams; ++i)
+      if (s->stream_last[i] < s->stream_last[si]) si = i;
+    s->stream_last[si] = Clock::now();
+    r->inst = inst;
+    r->stream = si;
+    cudaStream_t st = s->streams[si];
+    lk.unlock();
+    cudaError_t e = cudaMallocFromPoolAsync(&r->d_in, r->bytes, s->pool, st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&r->d_out, r->bytes, s->pool, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r->d_in, r->host_in, r->bytes, cudaMemcpyHostToDevice, st);
+    int xrc = 0;
+    if (e == cudaSuccess)
+      xrc = shafft_sm100_execute(inst->plan, r->d_in, r->d_out, r->direction, r->scale, st);
+    if (e == cudaSuccess && !xrc)
+      e = cudaMemcpyAsync(r->host_out, r->d_out, r->bytes, cudaMemcpyDeviceToHost, st);
+    if (r->d_in) cudaFreeAsync(r->d_in, st);
+    if (r->d_out) cudaFreeAsync(r->d_out, st);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(r->ev, st);
+    lk.lock();
+    if (e != cudaSuccess || xrc) {
+      r->status = xrc ? xrc : sfail(SHAFFT_SM100_ECUDA, "issue: %s", cudaGetErrorString(e));
+      cudaStreamSynchronize(st);
+      r->done = true;
+      r->t_done = Clock::now();
+      s->used -= need;
+      inst->busy = false;
+      s->failed++;
+      s->cv_done.notify_all();
+      continue;
+    }
+    s->inflight.push_back(r);
+    s->max_inflight_seen = std::max<int>(s->max_inflight_seen, (int)s->inflight.size());
+  }
+}
+
+void completer_loop(shafft_sm100_server_s* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop || !s->inflight.empty()) {
+    bool any = false;
+    for (size_t i = 0; i < s->inflight.size();) {
+      auto r = s->inflight[i];
+      const cudaError_t q = cudaEventQuery(r->ev);
+      if (q == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      r->t_done = Clock::now();
+      if (q != cudaSuccess) {
+        r->status = sfail(SHAFFT_SM100_ECUDA, "request %llu: %s", (unsigned long long)r->id,
+                          cudaGetErrorString(q));
+        s->failed++;
+      } else {
+        s->completed++;
+        s->latencies_ms.push_back(
+            std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+        if (s->completed == 1) s->t_first = r->t_submit;
+        s->t_last = r->t_done;
+      }
+      cudaEventDestroy(r->ev);
+      r->ev = nullptr;
+      s->used -= 2 * r->bytes;
+      r->inst->busy = false;
+      r->inst->last_used = Clock::now();
+      r->done = true;
+      s->inflight.erase(s->inflight.begin() + i);
+      any = true;
+    }
+    if (any) {
+      s->cv_done.notify_all();
+      s->cv_queue.notify_all();
+    }
+    lk.unlock();
+    std::this_thread::sleep_for(std::chrono::microseconds(any ? 0 : 20));
+    lk.lock();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, int streams) {
+  if (!out || budget_bytes == 0 || streams < 1 || streams > 64)
+    return sfail(SHAFFT_SM100_EINVAL, "bad server arguments");
+  *out = nullptr;
+  auto* s = new (std::nothrow) shafft_sm100_server_s();
+  if (!s) return sfail(SHAFFT_SM100_EALLOC, "host allocation failed");
+  s->budget = budget_bytes;
+  s->nstreams = streams;
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&s->pool, s->device);
+  if (e == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;  // keep freed blocks cached in the pool
+    e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  for (int i = 0; e == cudaSuccess && i < streams; ++i) {
+    cudaStream_t st = nullptr;
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    s->streams.push_back(st);
+    s->stream_last.push_back(Clock::now());
+  }
+  if (e != cudaSuccess) {
+    for (auto st : s->streams)
+      if (st) cudaStreamDestroy(st);
+    delete s;
+    return sfail(SHAFFT_SM100_ECUDA, "server set-up: %s", cudaGetErrorString(e));
+  }
+  s->dispatcher = std::thread(dispatcher_loop, s);
+  s->completer = std::thread(completer_loop, s);
+  *out = s;
+  return 0;
+}
+
+int shafft_sm100_server_submit(shafft_sm100_server s, int ndim, const int64_t* dims, int precision,
+                               int direction, double scale, const void* host_in, void* host_out,
+                               uint64_t* id) {
+  if (!s || !dims || ndim < 1 || !host_in || !host_out || !id)
+    return sfail(SHAFFT_SM100_EINVAL, "bad request");
+  if (precision != 0 && precision != 1) return sfail(SHAFFT_SM100_EINVAL, "bad precision");
+  auto r = std::make_shared<Request>();
+  r->dims.assign(dims, dims + ndim);
+  int64_t n = 1;
+  for (int a = 0; a < ndim; ++a) {
+    if (dims[a] < 1) return sfail(SHAFFT_SM100_EINVAL, "bad dims");
+    n *= dims[a];
+  }
+  r->precision = precision;
+  r->direction = direction;
+  r->scale = scale;
+  r->host_in = host_in;
+  r->host_out = host_out;
+  r->bytes = (size_t)n * (precision ? 16 : 8);
+  r->t_submit = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->id = s->next_id++;
+  *id = r->id;
+  s->all[r->id] = r;
+  s->queue.push_back(r);
+  s->cv_queue.notify_one();
+  return 0;
+}
+
+int shafft_sm100_server_wait(shafft_sm100_server s, uint64_t id, double* latency_ms) {
+  if (!s) return sfail(SHAFFT_SM100_EINVAL, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return sfail(SHAFFT_SM100_EINVAL, "unknown request %llu", (unsigned long long)id);
+  auto r = it->second;
+  s->cv_done.wait(lk, [&] { return r->done; });
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+  const int st = r->status;
+  s->all.erase(id);
+  return st;
+}
+
+int shafft_sm100_server_stats(shafft_sm100_server s, char* buf, int buflen) {
+  if (!s || !buf || buflen <= 0) return sfail(SHAFFT_SM100_EINVAL, "bad arguments");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::vector<double> v = s->latencies_ms;
+  std::sort(v.begin(), v.end());
+  auto pct = [&](double q) { return v.empty() ? 0.0 : v[std::min(v.size() - 1, (size_t)(q * (v.size() - 1) + 0.5))]; };
+  const double span = s->completed ? std::chrono::duration<double>(s->t_last - s->t_first).count() : 0;
+  snprintf(buf, buflen,
+           "{\"completed\":%llu,\"failed\":%llu,\"p50_ms\":%.4f,\"p99_ms\":%.4f,\"max_ms\":%.4f,"
+           "\"throughput_per_s\":%.3f,\"max_inflight\":%d,\"resident_plan_bytes\":%zu,\"streams\":%d}",
+           (unsigned long long)s->completed, (unsigned long long)s->failed, pct(0.5), pct(0.99),
+           v.empty() ? 0.0 : v.back(), span > 0 ? s->completed / span : 0.0, s->max_inflight_seen,
+           s->plan_bytes, s->nstreams);
+  return 0;
+}
+
+int shafft_sm100_server_reset_stats(shafft_sm100_server s) {
+  if (!s) return sfail(SHAFFT_SM100_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->latencies_ms.clear();
+  s->completed = s->failed = 0;
+  s->max_inflight_seen = 0;
+  return 0;
+}
+
+int shafft_sm100_server_destroy(shafft_sm100_server s) {
+  if (!s) return 0;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv_queue.notify_all();
+  }
+  s->dispatcher.join();
+  s->completer.join();
+  for (auto st : s->streams) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  for (auto& kv : s->plans)
+    for (auto& p : kv.second) shafft_sm100_plan_destroy(p->plan);
+  delete s;
+  return 0;
+}
+
+}  // extern "C"
