@@ -112,18 +112,23 @@ std::string plan_key(const Request& r) {
   return k;
 }
 
-// caller holds s->mu; returns a free plan instance for r, creating one (and
-// evicting idle instances of other shapes if the budget needs it)
-PlanInst* acquire_plan(shafft_sm100_server_s* s, const Request& r, int* rc) {
-  auto& vec = s->plans[plan_key(r)];
-  for (auto& p : vec)
+// caller holds s->mu (locked in `lk`); returns a free plan instance for r,
+// creating one when every instance of the shape is busy.  Creation (device
+// allocations, table kernels, a synchronisation) runs with the lock released
+// so that completions keep flowing meanwhile.
+PlanInst* acquire_plan(shafft_sm100_server_s* s, std::unique_lock<std::mutex>& lk, const Request& r,
+                       int* rc) {
+  const std::string key = plan_key(r);
+  for (auto& p : s->plans[key])
     if (!p->busy) {
       p->busy = true;
       p->last_used = Clock::now();
       return p.get();
     }
+  lk.unlock();
   shafft_sm100_plan pl = nullptr;
   *rc = shafft_sm100_plan_create_nd(&pl, (int)r.dims.size(), r.dims.data(), r.precision);
+  lk.lock();
   if (*rc) return nullptr;
   auto inst = std::make_unique<PlanInst>();
   inst->plan = pl;
@@ -132,14 +137,19 @@ PlanInst* acquire_plan(shafft_sm100_server_s* s, const Request& r, int* rc) {
   inst->last_used = Clock::now();
   s->plan_bytes += inst->bytes;
   s->used += inst->bytes;
+  auto& vec = s->plans[key];
   vec.push_back(std::move(inst));
   return vec.back().get();
 }
 
-// caller holds s->mu: drop idle plan instances, oldest first, until `need`
-// more bytes fit the budget
-void evict_idle(shafft_sm100_server_s* s, size_t need) {
-  while (s->used + need > s->budget) {
+// caller holds s->mu: unlink idle plan instances, oldest first, until the
+// resident plans leave room for `need` bytes.  Buffers of requests in flight
+// are not counted: they come back as those requests complete, so waiting for
+// them is cheaper than destroying and later re-creating plans.  The unlinked plans are returned in `dead` and
+// destroyed by the caller after it drops the lock (cudaFree synchronises the
+// device, which must not happen while completions wait for the lock).
+void evict_idle(shafft_sm100_server_s* s, size_t need, std::vector<shafft_sm100_plan>& dead) {
+  while (s->plan_bytes + need > s->budget) {
     PlanInst* victim = nullptr;
     std::string vkey;
     for (auto& kv : s->plans)
@@ -152,7 +162,7 @@ void evict_idle(shafft_sm100_server_s* s, size_t need) {
     auto& vec = s->plans[vkey];
     for (size_t i = 0; i < vec.size(); ++i)
       if (vec[i].get() == victim) {
-        shafft_sm100_plan_destroy(victim->plan);
+        dead.push_back(victim->plan);
         s->plan_bytes -= victim->bytes;
         s->used -= victim->bytes;
         vec.erase(vec.begin() + i);
@@ -172,7 +182,15 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
     }
     std::shared_ptr<Request> r = s->queue.front();
     const size_t need = 2 * r->bytes;
-    if (s->used + need > s->budget) evict_idle(s, need);
+    if (s->plan_bytes + need > s->budget) {
+      std::vector<shafft_sm100_plan> dead;
+      evict_idle(s, need, dead);
+      if (!dead.empty()) {
+        lk.unlock();
+        for (auto pl : dead) shafft_sm100_plan_destroy(pl);
+        lk.lock();
+      }
+    }
     if (s->used + need > s->budget) {
       if (s->inflight.empty()) {
         // can never fit: fail it instead of blocking the queue
@@ -190,7 +208,7 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
     }
     s->queue.pop_front();
     int rc = 0;
-    PlanInst* inst = acquire_plan(s, *r, &rc);
+    PlanInst* inst = acquire_plan(s, lk, *r, &rc);
     if (!inst) {
       r->status = rc;
       r->done = true;
