@@ -52,9 +52,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dims", default=None, help="override the 512^3 workload (debug only)")
+    ap.add_argument("--tensor-core", action="store_true",
+                    help="plan with the tensor-core form (complex64; debug / profiling of that form)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--suite", default="headline", choices=["headline", "batched", "serve", "configs"],
+    ap.add_argument("--suite", default="headline", choices=["headline", "batched", "serve", "configs", "tc"],
                     help="headline (default, the contract line) or one of the side workloads")
     ap.add_argument("--count", type=int, default=4096, help="transforms of the batched suite")
     return ap.parse_args()
@@ -237,7 +239,7 @@ def ours(args):
 
     dims = tuple(int(v) for v in args.dims.split("x")) if args.dims else DIMS
     n = math.prod(dims)
-    plan = _sm100.Plan(dims, 0)
+    plan = _sm100.Plan(dims, 0, _sm100.PLAN_TENSOR_CORE if args.tensor_core else 0)
     nst = plan.launches
     scale = float(1.0 / math.sqrt(n))
     stream = torch.cuda.current_stream()
@@ -671,6 +673,86 @@ def suite_configs(args):
     return 0
 
 
+def suite_tc(args):
+    """Tensor-core form (tcgen05 split-FP16 DFT stages) against the plain
+    kernels on the same GPU: fwd+bwd time, per-pass kernel times and the
+    forward error of both forms against the FP64 oracle."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as o
+    from shafft_b200 import _sm100
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.current_stream()
+    peak, _ = peaks()
+    res = []
+
+    def run(dims, flags, reps, ref):
+        n = math.prod(dims)
+        x = o.uniform_input(dims, seed=42, dtype=np.complex64)
+        a = torch.from_numpy(x.ravel()).cuda()
+        b = torch.empty_like(a)
+        p = _sm100.Plan(dims, 0, flags)
+        p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+        p.status()
+        err = o.rel_l2(b.cpu().numpy(), ref.ravel())
+        a.copy_(torch.from_numpy(x.ravel()))
+        for _ in range(3):
+            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+            p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+            p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        # per-launch times of one forward (steps run in order on one stream)
+        steps = p.describe()["steps"]
+        per = []
+        for i in range(p.launches):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            for _ in range(2):
+                p.execute_step(i, a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+            s0.record(stream)
+            for _ in range(5):
+                p.execute_step(i, a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            t = s0.elapsed_time(s1) / 5
+            st = steps[i]
+            d = {"kind": st["kind"], "L": st.get("L"), "tc": st.get("tc", 0), "ms": t,
+                 "gbs": p.step_bytes(i) / (t / 1e3) / 1e9}
+            if st.get("tc"):
+                lp = (st["L"] + 15) // 16 * 16
+                rows = n // st["L"]
+                groups = -(-rows // 128)
+                # 3 products x Lp/16 K-steps x 4 MMAs of 128 x Lp x 16 per group
+                d["mma_tflops"] = groups * 3072 * lp * lp / (t / 1e3) / 1e12
+            per.append(d)
+        plan_bytes = sum(p.step_bytes(i) for i in range(p.launches))
+        out = {"ms_fwd_bwd": ms, "compulsory_gbs": 2 * 2 * 8 * n / (ms / 1e3) / 1e9,
+               "plan_gbs": 2 * plan_bytes / (ms / 1e3) / 1e9,
+               "pct_hbm_plan": 100 * 2 * plan_bytes / (ms / 1e3) / 1e9 / peak,
+               "launches": p.launches, "rel_l2_fwd_vs_fp64_oracle": err, "steps": per}
+        del a, b
+        p.destroy()
+        return out
+
+    for dims in ((1 << 24,), (1488375,), (1000003,), (64, 64, 32), (512, 512, 512)):
+        n = math.prod(dims)
+        x = o.uniform_input(dims, seed=42, dtype=np.complex64)
+        ref = o.fftn(x.astype(np.complex128))
+        plain = run(dims, 0, 10, ref)
+        tc = run(dims, _sm100.PLAN_TENSOR_CORE, 10, ref)
+        res.append({"dims": list(dims), "tol": 1e-6 * math.log2(n), "plain": plain, "tensor_core": tc,
+                    "speedup_tc_vs_plain": plain["ms_fwd_bwd"] / tc["ms_fwd_bwd"]})
+    print(json.dumps({"metric": "tensor-core split-FP16 form vs plain FP32 kernels, complex64 fwd+bwd",
+                      "configs": res, "data": "synthetic, iid uniform[-1,1) seed 42"}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -681,6 +763,8 @@ def main():
         return suite_serve(args)
     if args.suite == "configs":
         return suite_configs(args)
+    if args.suite == "tc":
+        return suite_tc(args)
     return ours(args)
 
 

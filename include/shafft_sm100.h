@@ -52,6 +52,17 @@ typedef struct shafft_sm100_plan_s* shafft_sm100_plan;
 int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t* dims,
                                 int precision);
 
+/* Plan flags for shafft_sm100_plan_create_nd_ex / shafft_sm100_plan_query_ex.
+ * SHAFFT_SM100_PLAN_TENSOR_CORE: complex64 only.  Every pass of length <= 64
+ * runs on the tensor cores (tcgen05 MMA, split FP16 hi/lo operands, FP32
+ * accumulation, per-row power-of-two scaling); axes are factored into at
+ * most 4 (1-D) or 3 (inner axes) such passes, anything else keeps the plain
+ * kernels.  No counterpart in the reference (its GPU path is hipFFT). */
+#define SHAFFT_SM100_PLAN_TENSOR_CORE 1
+
+int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64_t* dims,
+                                   int precision, int flags);
+
 /* Plan a 1-D C2C transform of length n (equivalent to the 1-D ND plan). */
 int shafft_sm100_plan_create_1d(shafft_sm100_plan* out, int64_t n, int precision);
 
@@ -93,6 +104,9 @@ size_t shafft_sm100_plan_device_bytes(shafft_sm100_plan plan);
 /* Host-only planning query (no device needed): writes a JSON description of
  * the pass list for the given shape into buf.  Returns the status code. */
 int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* buf, int buflen);
+/* Same, for a plan created with `flags` (SHAFFT_SM100_PLAN_*). */
+int shafft_sm100_plan_query_ex(int ndim, const int64_t* dims, int precision, int flags, char* buf,
+                               int buflen);
 
 /* Run only step `step` (0 <= step < plan_launches()) of an execute with the
  * same buffer roles as shafft_sm100_execute.  Running steps 0..n-1 in order

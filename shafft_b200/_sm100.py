@@ -34,6 +34,10 @@ def load():
     vp = ctypes.c_void_p
     i64p = ctypes.POINTER(ctypes.c_int64)
     lib.shafft_sm100_plan_create_nd.argtypes = [ctypes.POINTER(vp), ctypes.c_int, i64p, ctypes.c_int]
+    lib.shafft_sm100_plan_create_nd_ex.argtypes = [ctypes.POINTER(vp), ctypes.c_int, i64p, ctypes.c_int,
+                                                   ctypes.c_int]
+    lib.shafft_sm100_plan_query_ex.argtypes = [ctypes.c_int, i64p, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_char_p, ctypes.c_int]
     lib.shafft_sm100_plan_create_1d.argtypes = [ctypes.POINTER(vp), ctypes.c_int64, ctypes.c_int]
     lib.shafft_sm100_plan_destroy.argtypes = [vp]
     lib.shafft_sm100_set_stream.argtypes = [vp, vp]
@@ -81,27 +85,32 @@ def _check(rc, what):
         raise Sm100Error(f"{what} failed rc={rc}: {msg}")
 
 
-def plan_query(dims, precision=0) -> dict:
+# plan flags (shafft_sm100.h)
+PLAN_TENSOR_CORE = 1
+
+
+def plan_query(dims, precision=0, flags=0) -> dict:
     """Host-only planner query (no GPU needed)."""
     lib = load()
     d = (ctypes.c_int64 * len(dims))(*dims)
     buf = ctypes.create_string_buffer(1 << 16)
-    _check(lib.shafft_sm100_plan_query(len(dims), d, precision, buf, len(buf)), "plan_query")
+    _check(lib.shafft_sm100_plan_query_ex(len(dims), d, precision, flags, buf, len(buf)), "plan_query")
     return json.loads(buf.value.decode())
 
 
 class Plan:
     """Owning handle of a shafft_sm100 plan (device tables + scratch)."""
 
-    def __init__(self, dims, precision=0):
+    def __init__(self, dims, precision=0, flags=0):
         lib = load()
         self._lib = lib
         self.dims = tuple(int(x) for x in dims)
         self.precision = int(precision)
+        self.flags = int(flags)
         h = ctypes.c_void_p()
         d = (ctypes.c_int64 * len(self.dims))(*self.dims)
-        _check(lib.shafft_sm100_plan_create_nd(ctypes.byref(h), len(self.dims), d, self.precision),
-               "plan_create_nd")
+        _check(lib.shafft_sm100_plan_create_nd_ex(ctypes.byref(h), len(self.dims), d, self.precision,
+                                                  self.flags), "plan_create_nd")
         self.handle = h
 
     def execute(self, src_ptr: int, dst_ptr: int, direction: int = 0, scale: float = 1.0,
@@ -119,6 +128,11 @@ class Plan:
 
     def step_bytes(self, step: int) -> int:
         return int(self._lib.shafft_sm100_step_bytes(self.handle, int(step)))
+
+    def status(self):
+        """Synchronises and raises if a device-side wait of the last executes gave up."""
+        _check(self._lib.shafft_sm100_stream_sync(None), "stream_sync")
+        _check(self._lib.shafft_sm100_plan_status(self.handle), "plan_status")
 
     def describe(self) -> dict:
         buf = ctypes.create_string_buffer(1 << 16)

@@ -13,6 +13,16 @@ namespace shafft_sm100 {
 // shafft_sm100_last_error_message) and return `code`.
 int report_error(int code, const char* msg);
 
+// Tensor-core (tcgen05, split FP16) pass for complex64: one DFT stage of
+// length 2..64 over every row of the geometry g (tc.cu).  `err` is a device
+// int set to 1 when a wait for the tensor core gives up.
+bool tc_supported(const PassGeom& g);
+size_t tc_smem_bytes(int L);
+template <typename C>
+struct PassTables;
+int tc_pass(const PassGeom& g, const float2* in, float2* out, const PassTables<float2>& tb, int* err,
+            cudaStream_t s);
+
 template <typename T>
 struct Vec2;
 template <>

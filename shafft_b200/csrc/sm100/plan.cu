@@ -30,10 +30,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../../include/shafft_sm100.h"
@@ -95,6 +97,7 @@ struct Step {
   size_t smem = 0;
   int fast = 0;      // 1: specialised k_fft_fast pass (compile-time L)
   int fast_row = 0;  // specialised pass reads row tiles (transposing)
+  int tc = 0;        // 1: tensor-core pass (tcgen05 split-FP16 DFT GEMM, L <= 64)
   // ST_PLANE: g = X phase (src -> mid), g2 = Y phase (mid -> out)
   PassGeom g2{};
   int mid_buf = BUF_DST;
@@ -163,7 +166,15 @@ struct Planner {
   size_t table_bytes = 0;
   int64_t scratch_elems = 0;
 
-  explicit Planner(int prec) : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {
+  // tensor-core planning: every pass of length <= 64 is a tcgen05 pass
+  int tc_mode = 0;
+  bool cur_tc = false;  // set while the passes being built are tensor-core passes
+  size_t off_tcerr = 0;
+
+  explicit Planner(int prec, int flags = 0)
+      : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {
+    tc_mode = (prec == 0 && (flags & SHAFFT_SM100_PLAN_TENSOR_CORE)) ? 1 : 0;
+    if (tc_mode) off_tcerr = alloc(16);
     if (const char* e = getenv("SHAFFT_SM100_PLANE")) plane_enabled = atoi(e) != 0;
     if (const char* e = getenv("SHAFFT_SM100_FLOW_LAG")) flow_lag = std::max(1, atoi(e));
   }
@@ -189,6 +200,7 @@ struct Planner {
   }
   // turn a planned generic pass into a specialised one when it qualifies
   void try_fast(Step& st) {
+    if (cur_tc) return mark_tc(st);
     PassGeom& g = st.g;
     if (!fast_len(g.L) || g.tw_mode == TW_PRE) return;
     const bool in_row = (g.sn_in == 1);
@@ -198,6 +210,12 @@ struct Planner {
     st.fast_row = in_row ? 1 : 0;
     finish_geom(st, fast_w());
     st.smem = (size_t)g.L * 128;
+  }
+
+  void mark_tc(Step& st) {
+    st.tc = 1;
+    st.fast = 0;
+    st.smem = tc_smem_bytes(st.g.L);
   }
 
   size_t alloc(size_t bytes) {
@@ -286,6 +304,7 @@ struct Planner {
       g.ext[1] = g.ext[2] = g.ext[3] = 1;
       g.sn_in = g.sk_out = 1;
       finish_geom(st, W);
+      if (cur_tc) mark_tc(st);
     } else {
       int W = col_width(L, I);
       g.ext[0] = I;
@@ -453,7 +472,7 @@ struct Planner {
       g.sn_in = I;
       g.sk_out = (L / R) * I;
       // digit t: input stride m_t*I, output stride (L_0..L_{t-1})*I
-      int64_t din[2] = {0, 0}, dout[2] = {0, 0}, dext[2] = {1, 1};
+      int64_t din[3] = {0, 0, 0}, dout[3] = {0, 0, 0}, dext[3] = {1, 1, 1};
       int64_t prod = 1;
       for (int t = 0; t < S - 1; ++t) {
         prod *= Ls[t];
@@ -468,6 +487,12 @@ struct Planner {
         g.ext[2] = dext[1];  g.sin[2] = din[1];  g.sout[2] = dout[1];
         g.ext[3] = O;  g.sin[3] = g.sout[3] = L * I;
         W = col_width(R, I);
+      } else if (S == 4) {
+        g.ext[0] = dext[0];  g.sin[0] = din[0];  g.sout[0] = dout[0];
+        g.ext[1] = dext[1];  g.sin[1] = din[1];  g.sout[1] = dout[1];
+        g.ext[2] = dext[2];  g.sin[2] = din[2];  g.sout[2] = dout[2];
+        g.ext[3] = O;  g.sin[3] = g.sout[3] = L;
+        W = 1;
       } else {
         g.ext[0] = dext[0];  g.sin[0] = din[0];  g.sout[0] = dout[0];
         g.ext[1] = dext[1];  g.sin[1] = din[1];  g.sout[1] = dout[1];
@@ -502,9 +527,68 @@ struct Planner {
   }
 
   // Plan one axis; `cur` holds the data on entry and on exit.
+  // Factor L into S <= max_s factors, each in 2..64, as balanced as possible
+  // (largest smallest factor); empty if L has a prime factor above 64 or
+  // needs more factors.
+  static std::vector<int> tc_split(int64_t L, int max_s) {
+    std::vector<int> best;
+    for (int S = 2; S <= max_s && best.empty(); ++S) {
+      std::vector<int> cur;
+      int best_min = 0;
+      // depth-first over non-increasing factor sequences
+      std::function<void(int64_t, int)> rec = [&](int64_t rem, int hi) {
+        const int k = (int)cur.size();
+        if (k == S - 1) {
+          if (rem >= 2 && rem <= hi) {
+            cur.push_back((int)rem);
+            const int mn = *std::min_element(cur.begin(), cur.end());
+            if (mn > best_min) {
+              best_min = mn;
+              best = cur;
+            }
+            cur.pop_back();
+          }
+          return;
+        }
+        for (int f = hi; f >= 2; --f) {
+          if (rem % f) continue;
+          cur.push_back(f);
+          rec(rem / f, f);
+          cur.pop_back();
+        }
+      };
+      rec(L, 64);
+    }
+    // multi_pass runs factors first-to-last; the last one is the row pass
+    std::reverse(best.begin(), best.end());
+    return best;
+  }
+
+  // Tensor-core route for one axis; false when the axis needs the plain path.
+  bool tc_axis(std::vector<Step>& out, int64_t O, int64_t L, int64_t I, int& cur, bool force_oop) {
+    if (!tc_mode) return false;
+    if (L <= 64) {
+      cur_tc = true;
+      const int ob = force_oop ? other_buf(cur) : cur;
+      single_pass(out, O, (int)L, I, cur, ob);
+      cur_tc = false;
+      cur = ob;
+      return true;
+    }
+    std::vector<int> f = tc_split(L, I == 1 ? 4 : 3);
+    if (f.empty()) return false;
+    cur_tc = true;
+    const int x = force_oop ? other_buf(cur) : cur;
+    multi_pass(out, O, L, I, f, cur, x);
+    cur_tc = false;
+    cur = out.back().out_buf;
+    return true;
+  }
+
   int axis(std::vector<Step>& out, int64_t O, int64_t L, int64_t I, int& cur, bool force_oop,
            bool in_bluestein) {
     if (L == 1) return 0;
+    if (tc_axis(out, O, L, I, cur, force_oop)) return 0;
     const int max_one = (I == 1) ? lim.max_row : lim.max_col;
     if (is_smooth(L) && L <= max_one) {
       int ob = force_oop ? other_buf(cur) : cur;
@@ -581,7 +665,7 @@ struct Planner {
     // the contiguous axis and its neighbour: two transposing passes when both
     // lengths have a specialised pass (every store is then a column tile)
     while (a >= 0 && dims[a] == 1) --a;
-    if (a >= 1) {
+    if (a >= 1 && !tc_mode) {
       int b = a - 1;
       while (b >= 0 && dims[b] == 1) --b;
       // only when the two axes are adjacent and some outer axis remains to
@@ -691,6 +775,8 @@ struct shafft_sm100_plan_s {
   void* d_s1 = nullptr;
   cudaStream_t stream = nullptr;
   int device = 0;
+  int flags = 0;
+  size_t off_tcerr = 0;  // tensor-core passes: device error word (0 = ok)
 };
 
 namespace {
@@ -745,6 +831,15 @@ struct Launcher {
       const NTable& nt = p->ntabs[st.tabN];
       g.tw_shift = nt.shift;
       g.tw_mask = nt.mask;
+    }
+    if (st.tc) {
+      if constexpr (std::is_same<T, float>::value) {
+        int* err = reinterpret_cast<int*>(p->d_tables + p->off_tcerr);
+        return tc_pass(g, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), tables(p, st),
+                       err, s);
+      } else {
+        return set_err(SHAFFT_SM100_ENOTSUP, "tensor-core pass on a complex128 plan");
+      }
     }
     if (st.fast)
       return check(K::fast(g, st.fast_row != 0, reinterpret_cast<const C*>(in),
@@ -874,11 +969,11 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
       snprintf(b, sizeof(b),
                "{\"kind\":\"pass\",\"L\":%d,\"radices\":[%s],\"W\":%d,\"in\":\"%s\",\"out\":\"%s\","
                "\"in_row\":%d,\"out_row\":%d,\"tiles\":%lld,\"smem\":%zu,\"twiddle\":%d,"
-               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d}",
+               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d,\"tc\":%d}",
                st.g.L, rad.c_str(), st.g.W, buf_name(st.in_buf), buf_name(st.out_buf), st.g.in_row,
                st.g.out_row, (long long)st.g.ntiles, st.smem, st.g.tw_mode, (long long)st.g.ext[0],
                (long long)st.g.ext[1], (long long)st.g.ext[2], (long long)st.g.ext[3],
-               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast);
+               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast, st.tc);
     } else {
       const char* k = st.kind == ST_BS_MOD    ? "bluestein_modulate"
                       : st.kind == ST_BS_MULH ? "bluestein_multiply"
@@ -906,6 +1001,13 @@ int copy_out(const std::string& s, char* buf, int buflen) {
   return 0;
 }
 
+int validate_flags(int flags, int precision) {
+  if (flags & ~SHAFFT_SM100_PLAN_TENSOR_CORE) return set_err(SHAFFT_SM100_EINVAL, "unknown plan flags");
+  if ((flags & SHAFFT_SM100_PLAN_TENSOR_CORE) && precision != 0)
+    return set_err(SHAFFT_SM100_ENOTSUP, "the tensor-core form is complex64 only");
+  return 0;
+}
+
 int validate_dims(int ndim, const int64_t* dims, int precision, int64_t* total) {
   if (ndim < 1 || ndim > 64 || !dims) return set_err(SHAFFT_SM100_EINVAL, "bad ndim/dims");
   if (precision != 0 && precision != 1) return set_err(SHAFFT_SM100_EINVAL, "bad precision");
@@ -924,10 +1026,17 @@ int validate_dims(int ndim, const int64_t* dims, int precision, int64_t* total) 
 extern "C" {
 
 int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* buf, int buflen) {
+  return shafft_sm100_plan_query_ex(ndim, dims, precision, 0, buf, buflen);
+}
+
+int shafft_sm100_plan_query_ex(int ndim, const int64_t* dims, int precision, int flags, char* buf,
+                               int buflen) {
   int64_t total = 0;
-  int rc = validate_dims(ndim, dims, precision, &total);
+  int rc = validate_flags(flags, precision);
   if (rc) return rc;
-  Planner pl(precision);
+  rc = validate_dims(ndim, dims, precision, &total);
+  if (rc) return rc;
+  Planner pl(precision, flags);
   std::vector<Step> steps;
   rc = pl.plan_nd(steps, ndim, dims);
   if (rc) return rc;
@@ -935,10 +1044,17 @@ int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* 
 }
 
 int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t* dims, int precision) {
+  return shafft_sm100_plan_create_nd_ex(out, ndim, dims, precision, 0);
+}
+
+int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64_t* dims,
+                                   int precision, int flags) {
   if (!out) return set_err(SHAFFT_SM100_EINVAL, "null plan pointer");
   *out = nullptr;
   int64_t total = 0;
-  int rc = validate_dims(ndim, dims, precision, &total);
+  int rc = validate_flags(flags, precision);
+  if (rc) return rc;
+  rc = validate_dims(ndim, dims, precision, &total);
   if (rc) return rc;
   std::unique_ptr<shafft_sm100_plan_s> p(new (std::nothrow) shafft_sm100_plan_s());
   if (!p) return set_err(SHAFFT_SM100_EALLOC, "host allocation failed");
@@ -946,9 +1062,11 @@ int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t*
   p->ndim = ndim;
   p->dims.assign(dims, dims + ndim);
   p->total = total;
-  Planner pl(precision);
+  p->flags = flags;
+  Planner pl(precision, flags);
   rc = pl.plan_nd(p->steps, ndim, dims);
   if (rc) return rc;
+  p->off_tcerr = pl.off_tcerr;
   p->ltabs = pl.ltabs;
   p->ntabs = pl.ntabs;
   p->btabs = pl.btabs;
@@ -967,6 +1085,13 @@ int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t*
       if (p->d_s0) cudaFree(p->d_s0);
       return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for scratch failed", b);
     }
+  }
+  if (cudaMemset(p->d_tables, 0, p->table_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(p->d_tables);
+    if (p->d_s0) cudaFree(p->d_s0);
+    if (p->d_s1) cudaFree(p->d_s1);
+    return set_err(SHAFFT_SM100_ECUDA, "cudaMemset of the plan tables failed");
   }
   rc = precision ? Launcher<double>::build_tables(p.get()) : Launcher<float>::build_tables(p.get());
   if (rc) {
@@ -1061,6 +1186,12 @@ int shafft_sm100_scale(void* data, size_t count, int precision, double factor, v
 
 int shafft_sm100_plan_status(shafft_sm100_plan plan) {
   if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
+  if (plan->flags & SHAFFT_SM100_PLAN_TENSOR_CORE) {
+    int flag = 0;
+    CUDA_TRY(cudaMemcpy(&flag, plan->d_tables + plan->off_tcerr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag)
+      return set_err(SHAFFT_SM100_ECUDA, "tensor-core pass: a wait for the MMA results timed out");
+  }
   for (const Step& st : plan->steps) {
     if (st.kind != ST_PLANE) continue;
     int flag = 0;
