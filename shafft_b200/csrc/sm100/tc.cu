@@ -258,8 +258,8 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     for (int j = 0; j < 8; j += 2) {
       float2 w0 = {0.f, 0.f}, w1 = {0.f, 0.f};
       const int n0 = 8 * c + j;
-      if (k < L && n0 < L) w0 = tb.twL[(int)(((int64_t)n0 * k) % L)];
-      if (k < L && n0 + 1 < L) w1 = tb.twL[(int)(((int64_t)(n0 + 1) * k) % L)];
+      if (k < L && n0 < L) w0 = __ldg(tb.twL + (n0 * k) % L);  // n, k < 64: 32-bit
+      if (k < L && n0 + 1 < L) w1 = __ldg(tb.twL + ((n0 + 1) * k) % L);
       split2(w0.x, w1.x, rh[j / 2], rl[j / 2]);
       split2(w0.y, w1.y, ih[j / 2], il[j / 2]);
     }
