@@ -242,7 +242,9 @@ def ours(args):
     plan = _sm100.Plan(dims, 0, _sm100.PLAN_TENSOR_CORE if args.tensor_core else 0)
     nst = plan.launches
     scale = float(1.0 / math.sqrt(n))
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the kernels and the events that time them share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     gen = torch.Generator(device="cuda").manual_seed(42 + rank)
     a = (torch.rand(2 * n, device="cuda", generator=gen) * 2 - 1).view(torch.complex64)
@@ -346,21 +348,33 @@ def ours(args):
 def e2e_arm(S, dims, n, args, stream, barrier, dist):
     """Public SHAFFT C ABI with host buffers: per step, copy the input from
     pinned host memory, forward+normalize, backward+normalize, copy the
-    result back."""
+    result back.  Two plan instances are driven from two host threads (each
+    thread's NULL-stream work goes to its own stream), so one step's
+    device->host copy overlaps the next step's host->device copy on the
+    full-duplex PCIe link; every step still moves its own input and result."""
+    import threading
+
     import torch
-    plan = S.FFTND()
-    S.check(plan.init([1] * len(dims), list(dims), S.C2C), "init")
-    S.check(plan.plan(), "plan")
-    da = S.DeviceBuffer(n, S.C2C)
-    db = S.DeviceBuffer(n, S.C2C)
-    S.check(plan.set_buffers(da.ptr, db.ptr), "setBuffers")
-    host_in = torch.empty(2 * n, dtype=torch.float32, pin_memory=True)
-    host_in.uniform_(-1, 1)
-    host_out = torch.empty(2 * n, dtype=torch.float32, pin_memory=True)
+    lanes = 2
     lib = S.load()
     nbytes = 8 * n
+    plans, bufs, hosts = [], [], []
+    for _ in range(lanes):
+        plan = S.FFTND()
+        S.check(plan.init([1] * len(dims), list(dims), S.C2C), "init")
+        S.check(plan.plan(), "plan")
+        da = S.DeviceBuffer(n, S.C2C)
+        db = S.DeviceBuffer(n, S.C2C)
+        S.check(plan.set_buffers(da.ptr, db.ptr), "setBuffers")
+        host_in = torch.empty(2 * n, dtype=torch.float32, pin_memory=True)
+        host_in.uniform_(-1, 1)
+        host_out = torch.empty(2 * n, dtype=torch.float32, pin_memory=True)
+        plans.append(plan)
+        bufs.append((da, db))
+        hosts.append((host_in, host_out))
 
-    def step():
+    def step(i):
+        plan, (host_in, host_out) = plans[i], hosts[i]
         _, d, _ = plan.get_buffers()
         S.check(lib.shafftCopyToBufferF(ctypes.c_void_p(d), ctypes.c_void_p(host_in.data_ptr()), n),
                 "copyToBuffer")
@@ -370,31 +384,46 @@ def e2e_arm(S, dims, n, args, stream, barrier, dist):
         S.check(lib.shafftCopyFromBufferF(ctypes.c_void_p(host_out.data_ptr()), ctypes.c_void_p(d), n),
                 "copyFromBuffer")
 
-    for _ in range(max(2, min(args.warmup, 3))):
-        step()
-    k = max(3, min(args.steps, 10))
+    errors = []
+    dev = torch.cuda.current_device()  # new threads start on device 0
+
+    def lane(i, count):
+        try:
+            torch.cuda.set_device(dev)
+            for _ in range(count):
+                step(i)
+        except Exception as e:  # surfaced after join
+            errors.append(e)
+
+    def run(count_per_lane):
+        th = [threading.Thread(target=lane, args=(i, count_per_lane)) for i in range(lanes)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        if errors:
+            raise errors[0]
+
+    run(max(1, min(args.warmup, 2)))
+    k = lanes * max(2, min(args.steps, 10) // lanes)
     barrier()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(torch.cuda.default_stream())
     w0 = time.perf_counter()
-    for _ in range(k):
-        step()
-    t1.record(torch.cuda.default_stream())
+    run(k // lanes)
     barrier()
     wall = time.perf_counter() - w0
-    ms = t0.elapsed_time(t1)
-    tt = torch.tensor([max(ms, 1e3 * wall)], device="cuda", dtype=torch.float64)
+    tt = torch.tensor([1e3 * wall], device="cuda", dtype=torch.float64)
     if dist is not None:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
     tmax = float(tt.item())
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    plan.release()
+    for plan in plans:
+        plan.release()
     return {"value": world * step_bytes(dims) * k / (tmax / 1e3) / 1e9, "unit": UNIT,
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k,
             "ms_per_step": tmax / k,
             "path": "libshafft.so C ABI: shafftCopyToBufferF, shafftExecuteNormalized x2, "
-                    "shafftCopyFromBufferF, pinned host buffers"}
+                    "shafftCopyFromBufferF, pinned host buffers; 2 plans on 2 host threads "
+                    "(steps overlap), host wall clock between barriers"}
 
 
 # ---------------------------------------------------------------------------

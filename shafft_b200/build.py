@@ -28,8 +28,12 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 CXX = "g++"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
-                  "-I", INC]
+# Per-thread default stream: work a caller issues on the NULL stream (plan
+# default stream, synchronous copies) goes to the calling thread's own
+# stream, so plans driven from different host threads overlap; it still
+# synchronises with the legacy default stream other libraries use.
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--default-stream", "per-thread",
+                  "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-I", INC]
 CXXFLAGS = ["-O2", "-fPIC", "-std=c++17", "-Wall", "-Wextra", "-Wno-unused-parameter",
             "-I", INC, "-I", os.path.join(INC, "mpi_shim"), "-I", os.path.join(CUDA, "include")]
 
