@@ -214,23 +214,61 @@ def reference_arm(args):
 # our arm
 # ---------------------------------------------------------------------------
 
+# ---------------------------------------------------------------------------
+# replicas: one process per GPU, no data-path collective
+# ---------------------------------------------------------------------------
+
+def dist_init(backend="nccl"):
+    """(rank, world, local_rank, process group or None) from the torchrun
+    environment; the group exists only for N > 1 and carries timing
+    reductions, never data."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+    return rank, world, local, dist
+
+
+def _reduce(x, dist, device, op):
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op(dist))
+    return float(t.item())
+
+
+def max_over_ranks(x, dist, device="cuda"):
+    return _reduce(x, dist, device, lambda d: d.ReduceOp.MAX)
+
+
+def sum_over_ranks(x, dist, device="cuda"):
+    return _reduce(x, dist, device, lambda d: d.ReduceOp.SUM)
+
+
+def shard(seq, rank, world):
+    """Contiguous block of `seq` owned by `rank` (block sizes differ by at
+    most one; the blocks of all ranks partition `seq` in order)."""
+    n = len(seq)
+    return list(seq[rank * n // world:(rank + 1) * n // world])
+
+
 def ours(args):
     import torch
 
     import shafft_b200 as S
     from shafft_b200 import _sm100
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    rank, world, local, dist = dist_init("nccl")
 
     def barrier():
         if dist is not None:
@@ -281,10 +319,7 @@ def ours(args):
     bounds = [e for (_, _, e) in events] + [t1]
     for j, (direction, i, ev) in enumerate(events):
         per.setdefault(i, []).append(ev.elapsed_time(bounds[j + 1]))
-    tmax = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    tmax = float(tmax.item())
+    tmax = max_over_ranks(total_ms, dist)
     ms_per_step = tmax / args.steps
     value = world * step_bytes(dims) * args.steps / (tmax / 1e3) / 1e9
 
@@ -411,10 +446,7 @@ def e2e_arm(S, dims, n, args, stream, barrier, dist):
     run(k // lanes)
     barrier()
     wall = time.perf_counter() - w0
-    tt = torch.tensor([1e3 * wall], device="cuda", dtype=torch.float64)
-    if dist is not None:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    tmax = float(tt.item())
+    tmax = max_over_ranks(1e3 * wall, dist)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     for plan in plans:
         plan.release()
@@ -471,7 +503,9 @@ def suite_batched(args):
     from oracle import oracle as o
     from shafft_b200 import _sm100
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    shapes = batched_shapes(args.count)
+    rank, world, _, dist = dist_init("nccl")
+    # replicas: each rank owns a contiguous block of the transform list
+    shapes = shard(batched_shapes(args.count), rank, world)
     sizes = [math.prod(s) for s in shapes]
     offs, tot = [], 0
     for n in sizes:
@@ -532,11 +566,18 @@ def suite_batched(args):
     torch.cuda.synchronize()
     t_plain = e0.elapsed_time(e1) / 2
     comp = sum(2 * 8 * n for n in sizes)
+    # whole job: bytes of all ranks over the slowest rank's time
+    comp_all = sum_over_ranks(comp, dist)
+    t_batch = max_over_ranks(t_batch, dist)
+    t_plain = max_over_ranks(t_plain, dist)
+    if rank != 0:
+        dist.destroy_process_group()
+        return 0
     out = {
         "metric": "batched uneven 2-D/3-D c64 forward transforms: compulsory GB/s", "unit": "GB/s",
-        "value": comp / (t_batch / 1e3) / 1e9, "plain_value": comp / (t_plain / 1e3) / 1e9,
+        "value": comp_all / (t_batch / 1e3) / 1e9, "plain_value": comp_all / (t_plain / 1e3) / 1e9,
         "speedup_vs_plain": t_plain / t_batch, "ms_batched": t_batch, "ms_plain": t_plain,
-        "transforms": len(shapes), "elements": sum(sizes),
+        "n_gpus": world, "transforms_per_rank": len(shapes), "elements_rank0": sum(sizes),
         "plan_hbm_gbs_batched": batch.alg_bytes / (t_batch / 1e3) / 1e9,
         "launches_batched_per_execute": 1, "launches_plain_per_execute": launches,
         "create_s": {"batch_with_autotune": t_create, "plain_plans": t_plans},
@@ -544,6 +585,8 @@ def suite_batched(args):
         "tol_c64": "1e-6*log2(N)", "data": "synthetic",
     }
     print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
     return 0
 
 
@@ -579,7 +622,9 @@ def suite_serve(args):
 
     from shafft_b200 import _sm100
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    reqs = serve_requests(max(40, min(args.count, 400)))
+    rank, world, _, dist = dist_init("nccl")
+    # replicas: each rank serves a contiguous block of the request stream
+    reqs = shard(serve_requests(max(40, min(args.count, 400)) * world), rank, world)
     maxb = max(math.prod(d) * (16 if p else 8) for d, p, _ in reqs)
     hin = torch.empty(maxb // 4, dtype=torch.float32, pin_memory=True).uniform_(-1, 1)
     hout = torch.empty(maxb // 4, dtype=torch.float32, pin_memory=True)
@@ -639,11 +684,22 @@ def suite_serve(args):
         sweep.append(st)
     srv.destroy()
     best = max(s["achieved_per_s"] for s in sweep)
+    # whole job: request rates add over the replicas; latency is the worst rank's
+    best_all = sum_over_ranks(best, dist)
+    serial_all = sum_over_ranks(serial_tput, dist)
+    p99_best = max_over_ranks(max(sweep, key=lambda s: s["achieved_per_s"])["p99_ms"], dist)
+    if rank != 0:
+        dist.destroy_process_group()
+        return 0
     out = {"metric": "served mixed C2C requests: throughput and p50/p99 latency", "unit": "requests/s",
-           "value": best, "serial_plain": serial, "speedup_vs_serial": best / serial_tput,
-           "requests": len(reqs), "budget_bytes": 40 << 30, "streams": 8, "sweep": sweep,
+           "value": best_all, "serial_plain": serial, "speedup_vs_serial": best_all / serial_all,
+           "n_gpus": world, "p99_ms_at_best_worst_rank": p99_best,
+           "requests_per_rank": len(reqs), "budget_bytes": 40 << 30, "streams": 8,
+           "sweep_rank0": sweep,
            "host_buffers": "pinned, shared by all requests (timing only)", "data": "synthetic"}
     print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
     return 0
 
 
