@@ -177,6 +177,7 @@ struct Planner {
     if (tc_mode) off_tcerr = alloc(16);
     if (const char* e = getenv("SHAFFT_SM100_PLANE")) plane_enabled = atoi(e) != 0;
     if (const char* e = getenv("SHAFFT_SM100_FLOW_LAG")) flow_lag = std::max(1, atoi(e));
+    if (const char* e = getenv("SHAFFT_SM100_ROTATE")) rotate_enabled = atoi(e) != 0;
   }
 
   // specialised-pass eligibility: length, tile width and 16-byte alignment
@@ -658,8 +659,46 @@ struct Planner {
     return 0;
   }
 
+  // Rotation chain for an odd number (>= 3) of non-trivial axes: each pass
+  // transforms the contiguous axis (row tiles) and stores it as the slowest
+  // index (column tiles), so after one pass per axis the layout is natural
+  // again and every pass is a transposing pass; src -> dst -> ... -> dst.
+  bool rotation_chain(std::vector<Step>& out, int ndim, const int64_t* dims) {
+    std::vector<int64_t> ax;
+    int64_t N = 1;
+    for (int a = 0; a < ndim; ++a)
+      if (dims[a] > 1) {
+        ax.push_back(dims[a]);
+        N *= dims[a];
+      }
+    if (ax.size() < 3 || ax.size() % 2 == 0) return false;
+    std::vector<Step> tmp;
+    int cur = BUF_SRC;
+    for (int i = (int)ax.size() - 1; i >= 0; --i) {
+      const int64_t L = ax[i];
+      if (!fast_len(L) || (N / L) % fast_w()) return false;
+      Step st;
+      st.kind = ST_PASS;
+      st.in_buf = cur;
+      st.out_buf = other_buf(cur);
+      fill_radix(st.g, (int)L);
+      st.g.ext[0] = N / L;  st.g.sin[0] = L;  st.g.sout[0] = 1;
+      st.g.sn_in = 1;
+      st.g.sk_out = N / L;
+      finish_geom(st, fast_w());
+      try_fast(st);
+      if (!st.fast) return false;
+      tmp.push_back(st);
+      cur = other_buf(cur);
+    }
+    out = tmp;
+    return true;
+  }
+  int rotate_enabled = 0;  // SHAFFT_SM100_ROTATE=1: rotation chain for 3-D and odd-rank tensors
+
   int plan_nd(std::vector<Step>& out, int ndim, const int64_t* dims) {
     out.clear();
+    if (rotate_enabled && !tc_mode && rotation_chain(out, ndim, dims)) return 0;
     int cur = BUF_SRC;
     int a = ndim - 1;
     // the contiguous axis and its neighbour: two transposing passes when both

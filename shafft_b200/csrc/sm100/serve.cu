@@ -102,6 +102,9 @@ struct shafft_sm100_server_s {
   Clock::time_point t_first, t_last;
   uint64_t completed = 0, failed = 0;
   int max_inflight_seen = 0;
+  // plan-instance churn: creations (and their wall time) and evictions
+  uint64_t plans_created = 0, plans_evicted = 0;
+  double create_ms_total = 0, create_ms_max = 0;
 };
 
 namespace {
@@ -127,8 +130,13 @@ PlanInst* acquire_plan(shafft_sm100_server_s* s, std::unique_lock<std::mutex>& l
     }
   lk.unlock();
   shafft_sm100_plan pl = nullptr;
+  const auto t0 = Clock::now();
   *rc = shafft_sm100_plan_create_nd(&pl, (int)r.dims.size(), r.dims.data(), r.precision);
+  const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
   lk.lock();
+  s->plans_created++;
+  s->create_ms_total += ms;
+  s->create_ms_max = std::max(s->create_ms_max, ms);
   if (*rc) return nullptr;
   auto inst = std::make_unique<PlanInst>();
   inst->plan = pl;
@@ -163,6 +171,7 @@ void evict_idle(shafft_sm100_server_s* s, size_t need, std::vector<shafft_sm100_
     for (size_t i = 0; i < vec.size(); ++i)
       if (vec[i].get() == victim) {
         dead.push_back(victim->plan);
+        s->plans_evicted++;
         s->plan_bytes -= victim->bytes;
         s->used -= victim->bytes;
         vec.erase(vec.begin() + i);
@@ -386,10 +395,13 @@ int shafft_sm100_server_stats(shafft_sm100_server s, char* buf, int buflen) {
   const double span = s->completed ? std::chrono::duration<double>(s->t_last - s->t_first).count() : 0;
   snprintf(buf, buflen,
            "{\"completed\":%llu,\"failed\":%llu,\"p50_ms\":%.4f,\"p99_ms\":%.4f,\"max_ms\":%.4f,"
-           "\"throughput_per_s\":%.3f,\"max_inflight\":%d,\"resident_plan_bytes\":%zu,\"streams\":%d}",
+           "\"throughput_per_s\":%.3f,\"max_inflight\":%d,\"resident_plan_bytes\":%zu,\"streams\":%d,"
+           "\"plans_created\":%llu,\"plans_evicted\":%llu,\"plan_create_ms_total\":%.3f,"
+           "\"plan_create_ms_max\":%.3f}",
            (unsigned long long)s->completed, (unsigned long long)s->failed, pct(0.5), pct(0.99),
            v.empty() ? 0.0 : v.back(), span > 0 ? s->completed / span : 0.0, s->max_inflight_seen,
-           s->plan_bytes, s->nstreams);
+           s->plan_bytes, s->nstreams, (unsigned long long)s->plans_created,
+           (unsigned long long)s->plans_evicted, s->create_ms_total, s->create_ms_max);
   return 0;
 }
 
@@ -399,6 +411,8 @@ int shafft_sm100_server_reset_stats(shafft_sm100_server s) {
   s->latencies_ms.clear();
   s->completed = s->failed = 0;
   s->max_inflight_seen = 0;
+  s->plans_created = s->plans_evicted = 0;
+  s->create_ms_total = s->create_ms_max = 0;
   return 0;
 }
 
