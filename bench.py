@@ -260,6 +260,17 @@ def shard(seq, rank, world):
     return list(seq[rank * n // world:(rank + 1) * n // world])
 
 
+def kernel_name(st):
+    """Kernel that runs a plan step (from the plan's JSON description)."""
+    if st.get("tc"):
+        return "k_fft_tc"
+    if st.get("fast"):
+        return f"k_fft_fast<IN_ROW={st.get('in_row', 0)}>"
+    if st["kind"] == "plane":
+        return "k_fft_plane_flow"
+    return "k_fft_pass" if st["kind"] == "pass" else f"k_bs/{st['kind']}"
+
+
 def ours(args):
     import torch
 
@@ -335,7 +346,7 @@ def ours(args):
     traffic = committed_traffic(dims, "c64", dom["step"])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": f"k_fft_pass step {dom['step']} (L={dom['L']})",
+                "kernel": f"{kernel_name(desc['steps'][dom['step']])} step {dom['step']} (L={dom['L']})",
                 "alg_bytes_per_launch": dom["alg_bytes"]}
     plan_bytes_per_step = 2 * sum(k["alg_bytes"] for k in kern)
 
