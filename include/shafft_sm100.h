@@ -151,12 +151,14 @@ int shafft_sm100_batch_describe(shafft_sm100_batch b, char* buf, int buflen);
  * a dispatcher thread and a completion thread.  Requests (host input/output
  * buffers -- pinned for overlap) are admitted in arrival order as soon as
  * their two device buffers fit `budget_bytes` (resident plans count against
- * the budget; idle plans are evicted oldest first), issued on the least
- * recently used stream (H2D, execute, D2H) and so overlap with requests
- * already running.  wait() blocks until the request's output is in
- * host_out and returns its status and latency (submission to completion).
- * stats() reports completed / failed counts, p50 / p99 / max latency and
- * throughput as JSON.  Wait for every submitted request before destroy. */
+ * the budget; idle plans are evicted oldest first, and only when the
+ * resident plans alone leave no room), issued on the least recently used
+ * stream (H2D, execute, D2H) and so overlap with requests already running.
+ * wait() blocks until the request's output is in host_out and returns its
+ * status and latency (submission to completion).  stats() reports completed
+ * / failed counts, p50 / p99 / max latency, throughput and plan-instance
+ * creations / evictions as JSON.  Wait for every submitted request before
+ * destroy. */
 typedef struct shafft_sm100_server_s* shafft_sm100_server;
 int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, int streams);
 int shafft_sm100_server_submit(shafft_sm100_server s, int ndim, const int64_t* dims, int precision,
