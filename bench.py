@@ -836,14 +836,24 @@ def suite_tc(args):
         p.destroy()
         return out
 
-    for dims in ((1 << 24,), (1488375,), (1000003,), (64, 64, 32), (512, 512, 512)):
+    # the FFT1D sizes of the tensor-core configuration and the headline, then
+    # axes with a prime factor above 13, where the plain path runs O(L^2)
+    # direct DFTs and the hybrid plan (tensor cores on those axes only) applies
+    for dims in ((1 << 24,), (1488375,), (1000003,), (64, 64, 32), (512, 512, 512),
+                 (65536, 61), (65536, 47), (65536, 31), (65536, 17), (4096, 61, 16), (61, 61, 61),
+                 (53, 59, 61)):
         n = math.prod(dims)
         x = o.uniform_input(dims, seed=42, dtype=np.complex64)
         ref = o.fftn(x.astype(np.complex128))
         plain = run(dims, 0, 10, ref)
         tc = run(dims, _sm100.PLAN_TENSOR_CORE, 10, ref)
-        res.append({"dims": list(dims), "tol": 1e-6 * math.log2(n), "plain": plain, "tensor_core": tc,
-                    "speedup_tc_vs_plain": plain["ms_fwd_bwd"] / tc["ms_fwd_bwd"]})
+        row = {"dims": list(dims), "tol": 1e-6 * math.log2(n), "plain": plain, "tensor_core": tc,
+               "speedup_tc_vs_plain": plain["ms_fwd_bwd"] / tc["ms_fwd_bwd"]}
+        if any(s.get("tc") for s in _sm100.plan_query(dims, 0, _sm100.PLAN_TC_PRIME_AXES)["steps"]):
+            hy = run(dims, _sm100.PLAN_TC_PRIME_AXES, 10, ref)
+            row["tc_prime_axes"] = hy
+            row["speedup_hybrid_vs_plain"] = plain["ms_fwd_bwd"] / hy["ms_fwd_bwd"]
+        res.append(row)
     print(json.dumps({"metric": "tensor-core split-FP16 form vs plain FP32 kernels, complex64 fwd+bwd",
                       "configs": res, "data": "synthetic, iid uniform[-1,1) seed 42"}), flush=True)
     return 0

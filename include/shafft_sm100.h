@@ -59,6 +59,12 @@ int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t*
  * most 4 (1-D) or 3 (inner axes) such passes, anything else keeps the plain
  * kernels.  No counterpart in the reference (its GPU path is hipFFT). */
 #define SHAFFT_SM100_PLAN_TENSOR_CORE 1
+/* SHAFFT_SM100_PLAN_TC_PRIME_AXES: complex64 only.  Tensor-core passes only
+ * for axes whose length has a prime factor above 13 (where the plain path
+ * computes O(L^2) direct DFTs or Bluestein); every other axis keeps the
+ * plain specialised passes.  Ignored when SHAFFT_SM100_PLAN_TENSOR_CORE is
+ * also set.  No counterpart in the reference. */
+#define SHAFFT_SM100_PLAN_TC_PRIME_AXES 2
 
 int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64_t* dims,
                                    int precision, int flags);

@@ -87,6 +87,7 @@ def _check(rc, what):
 
 # plan flags (shafft_sm100.h)
 PLAN_TENSOR_CORE = 1
+PLAN_TC_PRIME_AXES = 2
 
 
 def plan_query(dims, precision=0, flags=0) -> dict:

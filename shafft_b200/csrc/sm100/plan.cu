@@ -173,7 +173,11 @@ struct Planner {
 
   explicit Planner(int prec, int flags = 0)
       : precision(prec), lim(limits_for(prec)), elem(prec ? 16 : 8) {
-    tc_mode = (prec == 0 && (flags & SHAFFT_SM100_PLAN_TENSOR_CORE)) ? 1 : 0;
+    // 1: every pass on the tensor cores; 2: only axes with a prime factor
+    // above 13 (where the plain path would run O(L^2) direct DFTs)
+    tc_mode = prec != 0 ? 0
+              : (flags & SHAFFT_SM100_PLAN_TENSOR_CORE) ? 1
+              : (flags & SHAFFT_SM100_PLAN_TC_PRIME_AXES) ? 2 : 0;
     if (tc_mode) off_tcerr = alloc(16);
     if (const char* e = getenv("SHAFFT_SM100_PLANE")) plane_enabled = atoi(e) != 0;
     if (const char* e = getenv("SHAFFT_SM100_FLOW_LAG")) flow_lag = std::max(1, atoi(e));
@@ -605,6 +609,7 @@ struct Planner {
   // Tensor-core route for one axis; false when the axis needs the plain path.
   bool tc_axis(std::vector<Step>& out, int64_t O, int64_t L, int64_t I, int& cur, bool force_oop) {
     if (!tc_mode) return false;
+    if (tc_mode == 2 && is_smooth(L)) return false;  // smooth axes keep the plain passes
     if (L <= 64) {
       cur_tc = true;
       const int ob = force_oop ? other_buf(cur) : cur;
@@ -741,7 +746,7 @@ struct Planner {
     // the contiguous axis and its neighbour: two transposing passes when both
     // lengths have a specialised pass (every store is then a column tile)
     while (a >= 0 && dims[a] == 1) --a;
-    if (a >= 1 && !tc_mode) {
+    if (a >= 1 && tc_mode != 1) {
       int b = a - 1;
       while (b >= 0 && dims[b] == 1) --b;
       // only when the two axes are adjacent and some outer axis remains to
@@ -1078,8 +1083,9 @@ int copy_out(const std::string& s, char* buf, int buflen) {
 }
 
 int validate_flags(int flags, int precision) {
-  if (flags & ~SHAFFT_SM100_PLAN_TENSOR_CORE) return set_err(SHAFFT_SM100_EINVAL, "unknown plan flags");
-  if ((flags & SHAFFT_SM100_PLAN_TENSOR_CORE) && precision != 0)
+  const int tc_flags = SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES;
+  if (flags & ~tc_flags) return set_err(SHAFFT_SM100_EINVAL, "unknown plan flags");
+  if ((flags & tc_flags) && precision != 0)
     return set_err(SHAFFT_SM100_ENOTSUP, "the tensor-core form is complex64 only");
   return 0;
 }
@@ -1262,7 +1268,7 @@ int shafft_sm100_scale(void* data, size_t count, int precision, double factor, v
 
 int shafft_sm100_plan_status(shafft_sm100_plan plan) {
   if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
-  if (plan->flags & SHAFFT_SM100_PLAN_TENSOR_CORE) {
+  if (plan->flags & (SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES)) {
     int flag = 0;
     CUDA_TRY(cudaMemcpy(&flag, plan->d_tables + plan->off_tcerr, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag)

@@ -166,3 +166,41 @@ def test_planner_pass_lists():
     for dims in ([63, 47, 31], [1 << 24], [4096, 3], [7, 11, 13, 17], [2, 3, 4, 5]):
         q = _sm100.plan_query(dims, 0)
         assert q["steps"][-1]["out"] == "dst", dims
+
+
+def test_planner_balanced_splits():
+    """Measured-faster splits: balanced specialised factors for complex64,
+    largest last factor for complex128, balanced generic pair otherwise."""
+    def lens(dims, prec=0, flags=0):
+        return [s["L"] for s in _sm100.plan_query(dims, prec, flags)["steps"] if s["kind"] == "pass"]
+    assert lens([1 << 24]) == [256, 256, 256]
+    assert lens([1 << 24], 1) == [64, 512, 512]
+    assert lens([1488375]) == [1215, 1225]
+    q = _sm100.plan_query([1000003], 0)
+    assert [s["L"] for s in q["steps"] if s["kind"] == "pass"] == [128] * 6
+
+
+def test_planner_tensor_core_modes():
+    """Tensor-core planning: every pass (flag 1) or only the axes with a prime
+    factor above 13 (flag 2); complex64 only; unknown flags refused."""
+    TC, PRIME = _sm100.PLAN_TENSOR_CORE, _sm100.PLAN_TC_PRIME_AXES
+    q = _sm100.plan_query([1 << 24], 0, TC)
+    assert [s["L"] for s in q["steps"]] == [64] * 4 and all(s["tc"] for s in q["steps"])
+    q = _sm100.plan_query([1488375], 0, TC)
+    assert sorted(s["L"] for s in q["steps"]) == [27, 35, 35, 45]
+    # hybrid: the prime axis on the tensor cores, the smooth ones plain
+    q = _sm100.plan_query([4096, 61, 16], 0, PRIME)
+    assert [(s["L"], s["tc"]) for s in q["steps"]] == [(16, 0), (61, 1), (64, 0), (64, 0)]
+    q = _sm100.plan_query([512, 512, 512], 0, PRIME)
+    assert not any(s["tc"] for s in q["steps"]) and all(s["fast"] for s in q["steps"])
+    q = _sm100.plan_query([53, 59, 61], 0, PRIME)
+    assert [s["L"] for s in q["steps"]] == [61, 59, 53] and all(s["tc"] for s in q["steps"])
+    assert q["steps"][-1]["out"] == "dst"
+    # primes above 64 keep the plain path (direct DFT or Bluestein)
+    q = _sm100.plan_query([97, 64], 0, PRIME)
+    assert not any(s.get("tc") for s in q["steps"])
+    for bad_prec, flags in ((1, TC), (1, PRIME)):
+        with pytest.raises(_sm100.Sm100Error):
+            _sm100.plan_query([64], bad_prec, flags)
+    with pytest.raises(_sm100.Sm100Error):
+        _sm100.plan_query([64], 0, 4)

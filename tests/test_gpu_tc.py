@@ -94,3 +94,25 @@ def test_tc_every_length_2_to_64():
         y = run(plan, x)
         ref = o.fftn(x.astype(np.complex128))
         assert o.rel_l2(y, ref) <= tol(x.size), L
+
+
+PRIME_SHAPES = [(4096, 61), (61, 61, 61), (53, 59, 61), (512, 61, 16), (17, 19, 23, 8), (8, 1024, 47),
+                (61 * 64 * 32,)]
+
+
+@pytest.mark.parametrize("dims", PRIME_SHAPES, ids=lambda d: "x".join(map(str, d)))
+def test_tc_prime_axes_hybrid_vs_oracle(dims):
+    """Hybrid mode: tensor-core passes on the axes with a prime factor above
+    13, plain passes elsewhere; both directions against the oracle."""
+    PRIME = _sm100.PLAN_TC_PRIME_AXES
+    q = _sm100.plan_query(dims, 0, PRIME)
+    assert any(s.get("tc") for s in q["steps"]), q
+    plan = _sm100.Plan(dims, 0, PRIME)
+    x = o.uniform_input(dims, seed=11, dtype=np.complex64)
+    n = x.size
+    y = run(plan, x)
+    ref = o.fftn(x.astype(np.complex128))
+    assert o.rel_l2(y, ref) <= tol(n), o.rel_l2(y, ref)
+    yb = run(plan, x, direction=1, scale=1.0 / n)
+    refb = o.fftn(x.astype(np.complex128), sign=1) / n
+    assert o.rel_l2(yb, refb) <= tol(n), o.rel_l2(yb, refb)
