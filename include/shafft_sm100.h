@@ -69,6 +69,13 @@ int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t*
 int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64_t* dims,
                                    int precision, int flags);
 
+/* Transform only the listed axes of the tensor dims[0..ndim) (the others are
+ * batch axes); naxes < 0 or axes == NULL selects every axis.  The per-stage
+ * subplans of a slab-decomposed transform use this, as the reference's
+ * fftndPlan(nta, ta, ...) does (src/cpp/fft/hipfft_method/fftnd_method.cpp:162-351). */
+int shafft_sm100_plan_create_axes(shafft_sm100_plan* out, int ndim, const int64_t* dims,
+                                  int precision, int flags, int naxes, const int* axes);
+
 /* Plan a 1-D C2C transform of length n (equivalent to the 1-D ND plan). */
 int shafft_sm100_plan_create_1d(shafft_sm100_plan* out, int64_t n, int precision);
 
@@ -113,6 +120,8 @@ int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* 
 /* Same, for a plan created with `flags` (SHAFFT_SM100_PLAN_*). */
 int shafft_sm100_plan_query_ex(int ndim, const int64_t* dims, int precision, int flags, char* buf,
                                int buflen);
+int shafft_sm100_plan_query_axes(int ndim, const int64_t* dims, int precision, int flags, int naxes,
+                                 const int* axes, char* buf, int buflen);
 
 /* Run only step `step` (0 <= step < plan_launches()) of an execute with the
  * same buffer roles as shafft_sm100_execute.  Running steps 0..n-1 in order
@@ -174,6 +183,19 @@ int shafft_sm100_server_wait(shafft_sm100_server s, uint64_t id, double* latency
 int shafft_sm100_server_stats(shafft_sm100_server s, char* buf, int buflen);
 int shafft_sm100_server_reset_stats(shafft_sm100_server s);
 int shafft_sm100_server_destroy(shafft_sm100_server s);
+
+/* ---- Slab exchange helpers (distributed N-D transforms) -----------------
+ * src / dst: device arrays, viewed as [outer][n] row-major complex elements.
+ * pack: dst = the nparts column blocks of src one after the other, block p =
+ * columns [start_p, start_p + len_p) of every row as an [outer][len_p]
+ * array, (len_p, start_p) the block partition of n (the first n % nparts
+ * blocks one element longer); unpack is the inverse.  Asynchronous on
+ * `stream`.  Replaces the subarray datatypes of the reference's
+ * MPI_Alltoallw exchange (src/cpp/slab_nd.cpp:23-56). */
+int shafft_sm100_pack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
+                             int precision, void* stream);
+int shafft_sm100_unpack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
+                               int precision, void* stream);
 
 /* Device memory and stream helpers, so that callers above this ABI need no
  * CUDA runtime of their own (they replace the reference's allocBufferT /

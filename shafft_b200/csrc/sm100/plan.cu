@@ -738,21 +738,28 @@ struct Planner {
   }
   int rotate_enabled = 0;  // SHAFFT_SM100_ROTATE=1: rotation chain for 3-D and odd-rank tensors
 
+  // axes to transform (bit a = axis a); the others are batch axes
+  uint64_t axes_mask = ~0ull;
+
   int plan_nd(std::vector<Step>& out, int ndim, const int64_t* dims) {
     out.clear();
-    if (rotate_enabled && !tc_mode && rotation_chain(out, ndim, dims)) return 0;
+    auto on = [&](int a) { return dims[a] > 1 && ((axes_mask >> a) & 1ull); };
+    const bool all_axes = (ndim >= 64) || ((~axes_mask) & ((1ull << ndim) - 1)) == 0;
+    if (rotate_enabled && !tc_mode && all_axes && rotation_chain(out, ndim, dims)) return 0;
     int cur = BUF_SRC;
     int a = ndim - 1;
     // the contiguous axis and its neighbour: two transposing passes when both
     // lengths have a specialised pass (every store is then a column tile)
-    while (a >= 0 && dims[a] == 1) --a;
+    while (a >= 0 && !on(a)) --a;
     if (a >= 1 && tc_mode != 1) {
       int b = a - 1;
       while (b >= 0 && dims[b] == 1) --b;
-      // only when the two axes are adjacent and some outer axis remains to
-      // absorb the buffer parity (the pair itself ends where it started)
+      // only when the two axes are adjacent and transformed, and some outer
+      // transformed axis remains to absorb the buffer parity (the pair itself
+      // ends where it started)
       int outer = 0;
-      for (int c = 0; c < b; ++c) outer += dims[c] > 1;
+      for (int c = 0; c < b; ++c) outer += on(c);
+      if (b >= 0 && !on(b)) b = -1;
       if (b >= 0 && b == a - 1 && outer > 0) {
         int64_t O = 1;
         for (int c = 0; c < b; ++c) O *= dims[c];
@@ -766,7 +773,7 @@ struct Planner {
       int64_t I = 1, O = 1;
       for (int b = a + 1; b < ndim; ++b) I *= dims[b];
       for (int b = 0; b < a; ++b) O *= dims[b];
-      if (dims[a] == 1) continue;
+      if (!on(a)) continue;
       int rc = axis(out, O, dims[a], I, cur, false, false);
       if (rc) return rc;
     }
@@ -1082,6 +1089,23 @@ int copy_out(const std::string& s, char* buf, int buflen) {
   return 0;
 }
 
+// axes to transform as a bit mask; naxes < 0 or axes == NULL: every axis
+int axes_mask(int ndim, int naxes, const int* axes, uint64_t* mask) {
+  if (naxes < 0 || !axes) {
+    *mask = ~0ull;
+    return 0;
+  }
+  if (ndim > 64) return set_err(SHAFFT_SM100_ENOTSUP, "an axis subset needs ndim <= 64");
+  uint64_t m = 0;
+  for (int i = 0; i < naxes; ++i) {
+    if (axes[i] < 0 || axes[i] >= ndim) return set_err(SHAFFT_SM100_EINVAL, "axis %d out of range", axes[i]);
+    if ((m >> axes[i]) & 1ull) return set_err(SHAFFT_SM100_EINVAL, "axis %d listed twice", axes[i]);
+    m |= 1ull << axes[i];
+  }
+  *mask = m;
+  return 0;
+}
+
 int validate_flags(int flags, int precision) {
   const int tc_flags = SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES;
   if (flags & ~tc_flags) return set_err(SHAFFT_SM100_EINVAL, "unknown plan flags");
@@ -1113,12 +1137,21 @@ int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* 
 
 int shafft_sm100_plan_query_ex(int ndim, const int64_t* dims, int precision, int flags, char* buf,
                                int buflen) {
+  return shafft_sm100_plan_query_axes(ndim, dims, precision, flags, -1, nullptr, buf, buflen);
+}
+
+int shafft_sm100_plan_query_axes(int ndim, const int64_t* dims, int precision, int flags, int naxes,
+                                 const int* axes, char* buf, int buflen) {
   int64_t total = 0;
   int rc = validate_flags(flags, precision);
   if (rc) return rc;
   rc = validate_dims(ndim, dims, precision, &total);
   if (rc) return rc;
+  uint64_t mask = 0;
+  rc = axes_mask(ndim, naxes, axes, &mask);
+  if (rc) return rc;
   Planner pl(precision, flags);
+  pl.axes_mask = mask;
   std::vector<Step> steps;
   rc = pl.plan_nd(steps, ndim, dims);
   if (rc) return rc;
@@ -1131,12 +1164,20 @@ int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t*
 
 int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64_t* dims,
                                    int precision, int flags) {
+  return shafft_sm100_plan_create_axes(out, ndim, dims, precision, flags, -1, nullptr);
+}
+
+int shafft_sm100_plan_create_axes(shafft_sm100_plan* out, int ndim, const int64_t* dims,
+                                  int precision, int flags, int naxes, const int* axes) {
   if (!out) return set_err(SHAFFT_SM100_EINVAL, "null plan pointer");
   *out = nullptr;
   int64_t total = 0;
   int rc = validate_flags(flags, precision);
   if (rc) return rc;
   rc = validate_dims(ndim, dims, precision, &total);
+  if (rc) return rc;
+  uint64_t mask = 0;
+  rc = axes_mask(ndim, naxes, axes, &mask);
   if (rc) return rc;
   std::unique_ptr<shafft_sm100_plan_s> p(new (std::nothrow) shafft_sm100_plan_s());
   if (!p) return set_err(SHAFFT_SM100_EALLOC, "host allocation failed");
@@ -1146,6 +1187,7 @@ int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64
   p->total = total;
   p->flags = flags;
   Planner pl(precision, flags);
+  pl.axes_mask = mask;
   rc = pl.plan_nd(p->steps, ndim, dims);
   if (rc) return rc;
   p->off_tcerr = pl.off_tcerr;

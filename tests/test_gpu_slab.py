@@ -1,0 +1,144 @@
+"""GPU parts of the distributed (slab-decomposed) FFTND: kernel-library plans
+over axis subsets, block pack/unpack, and the whole transform on two
+processes.  The two ranks share this run's one GPU; their kernels are
+independent (nothing on the device waits for the other rank) and the
+exchange goes through host memory on a gloo group.  Tolerances as in the
+other parity tests: 1e-6*log2(N) (C2C), 1e-14*log2(N) (Z2Z)."""
+import json
+import math
+import os
+import socket
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import shafft_b200 as S
+from oracle import oracle as o
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def tol(n, prec):
+    return (1e-6 if prec == S.C2C else 1e-14) * max(1.0, math.log2(max(n, 2)))
+
+
+@pytest.mark.parametrize("dims,axes", [((6, 40, 48), [1, 2]), ((64, 5, 7), [0]), ((8, 12, 10, 6), [1, 3]),
+                                       ((97, 33), [1]), ((16, 16), [])])
+@pytest.mark.parametrize("prec", [S.C2C, S.Z2Z])
+def test_axis_subset_plans_vs_oracle(dims, axes, prec):
+    from shafft_b200.slab import CudaOps
+    import torch
+    ops = CudaOps(prec)
+    dt = np.complex128 if prec == S.Z2Z else np.complex64
+    x = o.uniform_input(dims, seed=3, dtype=dt)
+    a = torch.from_numpy(x.ravel()).cuda()
+    b = torch.empty_like(a)
+    h = ops.plan(list(dims), axes)
+    ops.execute(h, a, b, S.FORWARD)
+    torch.cuda.synchronize()
+    y = b.cpu().numpy().reshape(dims)
+    ref = o.fft_axes(x.astype(np.complex128), axes, precise=(prec == S.Z2Z)) if axes else x
+    assert o.rel_l2(y, ref) <= tol(x.size, prec)
+    ops.destroy(h)
+
+
+@pytest.mark.parametrize("outer,n,P", [(6, 48, 2), (5, 7, 3), (1, 10, 4), (33, 64, 8)])
+def test_pack_unpack_blocks(outer, n, P):
+    from shafft_b200.slab import CudaOps, block_partition
+    import torch
+    ops = CudaOps(S.C2C)
+    x = o.uniform_input((outer, n), seed=1, dtype=np.complex64)
+    a = torch.from_numpy(x.ravel()).cuda()
+    b = torch.empty_like(a)
+    c = torch.empty_like(a)
+    ops.pack(a, b, outer, n, P)
+    ops.unpack(b, c, outer, n, P)
+    torch.cuda.synchronize()
+    want = np.concatenate([x[:, s:s + l].ravel() for l, s in (block_partition(n, P, p) for p in range(P))])
+    assert np.array_equal(b.cpu().numpy(), want)
+    assert np.array_equal(c.cpu().numpy(), x.ravel())
+
+
+WORKER = r'''
+import json, math, sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np, torch, torch.distributed as dist
+import shafft_b200 as S
+from shafft_b200 import slab
+from oracle import oracle as o
+cfg = json.loads(sys.argv[3])
+torch.cuda.set_device(0)
+dist.init_process_group("gloo")
+dims, prec, P = tuple(cfg["dims"]), cfg["prec"], cfg["P"]
+dt = np.complex128 if prec == S.Z2Z else np.complex64
+g = o.uniform_input(dims, seed=42, dtype=dt)
+ref = o.fftn(g.astype(np.complex128), precise=(prec == S.Z2Z))
+plan = slab.FFTND()
+assert plan.init([P] + [1] * (len(dims) - 1), dims, prec, None, cfg["policy"]) == 0
+assert plan.plan() == 0
+n = plan.alloc_size()
+tdt = torch.complex128 if prec == S.Z2Z else torch.complex64
+a = torch.zeros(n, dtype=tdt, device="cuda"); b = torch.zeros_like(a)
+assert plan.set_buffers(a, b) == 0
+_, sub, off = plan.get_layout(S.TENSOR_LAYOUT_INITIAL)
+sl = lambda sub, off: tuple(slice(q, q + s) for q, s in zip(off, sub))
+_, d, _ = plan.get_buffers(); d[:math.prod(sub)] = torch.from_numpy(np.ascontiguousarray(g[sl(sub, off)]).ravel()).cuda()
+assert plan.execute(S.FORWARD) == 0
+_, sub, off = plan.get_layout()
+_, d, _ = plan.get_buffers()
+y = d[:math.prod(sub)].cpu().numpy().reshape(sub)
+r = ref[sl(sub, off)]
+fwd_layout = [sub, off]
+err2 = float(np.sum(np.abs(y - r) ** 2)); ref2 = float(np.sum(np.abs(r) ** 2))
+assert plan.execute(S.BACKWARD) == 0
+assert plan.normalize() == 0
+_, sub, off = plan.get_layout()
+_, d, _ = plan.get_buffers()
+back = d[:math.prod(sub)].cpu().numpy().reshape(sub)
+bt2 = float(np.sum(np.abs(back - g[sl(sub, off)]) ** 2)); g2 = float(np.sum(np.abs(g[sl(sub, off)]) ** 2))
+plan.release()
+dist.destroy_process_group()
+json.dump({"err2": err2, "ref2": ref2, "bt2": bt2, "g2": g2, "fwd_layout": fwd_layout}, open(sys.argv[2], "w"))
+'''
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+@pytest.mark.parametrize("dims,prec,policy", [((64, 48, 40), S.C2C, S.LAYOUT_REDISTRIBUTED),
+                                              ((64, 48, 40), S.Z2Z, S.LAYOUT_INITIAL),
+                                              ((97, 36, 10), S.C2C, S.LAYOUT_INITIAL),
+                                              ((128, 96), S.C2C, S.LAYOUT_REDISTRIBUTED)])
+def test_distributed_fftnd_two_ranks(tmp_path, dims, prec, policy):
+    world = 2
+    script = tmp_path / "worker.py"
+    script.write_text(WORKER)
+    port = _free_port()
+    cfg = {"dims": list(dims), "prec": prec, "P": world, "policy": policy}
+    procs = []
+    for r in range(world):
+        env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
+                   RANK=str(r), LOCAL_RANK=str(r))
+        procs.append(subprocess.Popen([sys.executable, str(script), ROOT, str(tmp_path / f"r{r}.json"),
+                                       json.dumps(cfg)], env=env))
+    for p in procs:
+        assert p.wait(timeout=300) == 0
+    res = [json.loads((tmp_path / f"r{r}.json").read_text()) for r in range(world)]
+    n = math.prod(dims)
+    # global relative L2 error over both ranks' blocks
+    err = math.sqrt(sum(x["err2"] for x in res) / sum(x["ref2"] for x in res))
+    back = math.sqrt(sum(x["bt2"] for x in res) / sum(x["g2"] for x in res))
+    assert err <= tol(n, prec), err
+    assert back <= 2 * tol(n, prec), back
+    if policy == S.LAYOUT_REDISTRIBUTED:
+        # forward output: full axis 0, the last axis in blocks
+        assert all(x["fwd_layout"][0][0] == dims[0] for x in res)
+        assert sum(x["fwd_layout"][0][-1] for x in res) == dims[-1]
+    else:
+        assert sum(x["fwd_layout"][0][0] for x in res) == dims[0]

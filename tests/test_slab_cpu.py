@@ -1,0 +1,151 @@
+"""Distributed (slab-decomposed) FFTND on CPU: the orchestration of
+shafft_b200.slab.FFTND -- stage layouts, block packing, all-to-all counts,
+buffer swaps, output layout policies, normalisation -- run on 2 and 3 gloo
+ranks.  The device steps are replaced here by numpy (test infrastructure
+only; the library's own steps are CUDA kernels, tested on the GPU in
+tests/test_gpu_slab.py)."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from shafft_b200 import slab  # noqa: E402
+
+WORKER = r'''
+import json, math, os, sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np, torch, torch.distributed as dist
+import shafft_b200 as S
+from shafft_b200 import slab
+
+class NumpyOps:
+    """Stand-in for the CUDA steps: numpy FFTs over axis subsets and the same
+    block layout as shafft_sm100_pack_blocks."""
+    def plan(self, dims, axes): return (tuple(dims), tuple(axes))
+    def destroy(self, h): pass
+    def execute(self, h, src, dst, direction):
+        dims, axes = h
+        n = math.prod(dims)
+        x = src[:n].numpy().reshape(dims)
+        if direction == S.FORWARD:
+            y = np.fft.fftn(x, axes=axes)
+        else:
+            y = np.fft.ifftn(x, axes=axes) * math.prod(dims[a] for a in axes)
+        dst[:n] = torch.from_numpy(y.ravel())
+    def pack(self, src, dst, outer, n, P):
+        a = src[:outer * n].numpy().reshape(outer, n)
+        parts = [a[:, s:s + l].ravel() for l, s in (slab.block_partition(n, P, p) for p in range(P))]
+        dst[:outer * n] = torch.from_numpy(np.concatenate(parts))
+    def unpack(self, src, dst, outer, n, P):
+        out = np.empty((outer, n), dtype=np.complex128); pos = 0
+        for p in range(P):
+            l, s = slab.block_partition(n, P, p)
+            out[:, s:s + l] = src[pos:pos + outer * l].numpy().reshape(outer, l); pos += outer * l
+        dst[:outer * n] = torch.from_numpy(out.ravel())
+    def scale(self, data, count, f): data[:count] *= f
+    def alltoall(self, out, inp, oc, ic, group, world):
+        o = torch.view_as_real(out[:sum(oc)]).view(-1); i = torch.view_as_real(inp[:sum(ic)]).view(-1)
+        dist.all_to_all_single(o, i, [2 * c for c in oc], [2 * c for c in ic], group=group)
+
+cfg = json.loads(sys.argv[3])
+dist.init_process_group("gloo")
+rank, world = dist.get_rank(), dist.get_world_size()
+dims = tuple(cfg["dims"]); P = cfg["P"]
+rng = np.random.Generator(np.random.MT19937(5))
+g = rng.uniform(-1, 1, dims) + 1j * rng.uniform(-1, 1, dims)
+f = S.__dict__
+plan = slab.FFTND()
+rc = plan.init([P] + [1] * (len(dims) - 1), dims, S.Z2Z, None, cfg["policy"], device_ops=NumpyOps())
+assert rc == 0, rc
+assert plan.plan() == 0
+n = plan.alloc_size()
+a = torch.zeros(max(n, 1), dtype=torch.complex128); b = torch.zeros_like(a)
+assert plan.set_buffers(a, b) == 0
+rc, sub, off = plan.get_layout(S.TENSOR_LAYOUT_INITIAL)
+sl = tuple(slice(o, o + s) for o, s in zip(off, sub))
+loc = g[sl]
+_, d, _ = plan.get_buffers(); d[:loc.size] = torch.from_numpy(loc.ravel())
+assert plan.execute(S.FORWARD) == 0
+rc, sub, off = plan.get_layout(S.TENSOR_LAYOUT_CURRENT)
+_, d, _ = plan.get_buffers()
+y = d[:math.prod(sub)].numpy().reshape(sub)
+ref = np.fft.fftn(g)[tuple(slice(o, o + s) for o, s in zip(off, sub))]
+fwd_err = float(np.abs(y - ref).max() / np.abs(ref).max()) if y.size else 0.0
+cur_axes = plan.get_axes(S.TENSOR_LAYOUT_CURRENT)
+assert plan.execute(S.BACKWARD) == 0
+assert plan.normalize() == 0
+rc, sub, off = plan.get_layout(S.TENSOR_LAYOUT_CURRENT)
+_, d, _ = plan.get_buffers()
+back = d[:math.prod(sub)].numpy().reshape(sub)
+rt_err = float(np.abs(back - g[tuple(slice(o, o + s) for o, s in zip(off, sub))]).max()) if back.size else 0.0
+dist.destroy_process_group()
+json.dump({"rank": rank, "fwd_err": fwd_err, "rt_err": rt_err, "fwd_layout": [sub, off],
+           "axes": cur_axes}, open(sys.argv[2], "w"))
+'''
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _run(tmp_path, world, cfg):
+    script = tmp_path / "worker.py"
+    script.write_text(WORKER)
+    port = _free_port()
+    procs = []
+    for r in range(world):
+        env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
+                   RANK=str(r), LOCAL_RANK=str(r))
+        procs.append(subprocess.Popen([sys.executable, str(script), ROOT, str(tmp_path / f"r{r}.json"),
+                                       json.dumps(cfg)], env=env))
+    for p in procs:
+        assert p.wait(timeout=240) == 0
+    return [json.loads((tmp_path / f"r{r}.json").read_text()) for r in range(world)]
+
+
+@pytest.mark.parametrize("world,dims,policy", [
+    (2, (6, 5, 7), 0), (2, (6, 5, 7), 1), (3, (7, 4, 5), 0), (3, (8, 6), 1), (2, (4, 3, 2, 5), 0)])
+def test_slab_fftnd_on_gloo_ranks(tmp_path, world, dims, policy):
+    res = _run(tmp_path, world, {"dims": list(dims), "P": world, "policy": policy})
+    for o in res:
+        assert o["fwd_err"] < 1e-12, o
+        assert o["rt_err"] < 1e-12, o
+
+
+def test_inactive_rank_takes_part_with_empty_blocks(tmp_path):
+    """commDims product below the group size: the extra rank owns nothing."""
+    res = _run(tmp_path, 3, {"dims": [4, 3, 5], "P": 2, "policy": 0})
+    assert all(o["fwd_err"] < 1e-12 and o["rt_err"] < 1e-12 for o in res)
+
+
+def test_layout_bookkeeping_matches_reference_partition():
+    L = slab.SlabLayout((6, 5, 7), 3, 1)
+    assert L.sub == [[2, 5, 7], [6, 5, 2]] and L.off == [[2, 0, 0], [0, 0, 3]]
+    assert L.alloc_size() == 70
+    assert L.forward_counts() == ([30, 20, 20], [20, 20, 20])
+    assert [slab.block_partition(10, 4, r) for r in range(4)] == [(3, 0), (3, 3), (2, 6), (2, 8)]
+
+
+def test_init_validation():
+    import shafft_b200 as S
+    p = slab.FFTND()
+    assert p.init([1, 2], [8, 8]) == S.ERR_INVALID_DECOMP       # last axis distributed
+    p = slab.FFTND()
+    assert p.init([1], [8, 8]) == S.ERR_DIM_MISMATCH
+    p = slab.FFTND()
+    assert p.init([9, 1], [8, 8]) == S.ERR_INVALID_DECOMP       # more parts than rows
+    p = slab.FFTND()
+    assert p.init([2, 2, 1], [8, 8, 8]) == S.ERR_NOT_IMPL       # pencils
+    p = slab.FFTND()
+    assert p.init([2, 1], [8, 8]) == S.ERR_INVALID_DECOMP       # 2 parts, 1 process
+    p = slab.FFTND()
+    assert p.plan() == S.ERR_PLAN_NOT_INIT
