@@ -196,6 +196,12 @@ int shafft_sm100_pack_blocks(const void* src, void* dst, int64_t outer, int64_t 
                              int precision, void* stream);
 int shafft_sm100_unpack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
                                int precision, void* stream);
+/* data[k][c] *= exp(sign * 2*pi*i * ((col0 + c) * k mod N) / N) over a
+ * rows x cols array (phase reduced in integers, FP64 sincospi): the twiddle
+ * between the stages of the distributed four-step FFT1D (replaces the
+ * reference's fft1dTwiddleKernel, 1d/fft1d_cooley_tukey_executor.hip:57-83). */
+int shafft_sm100_twiddle_rows(void* data, int64_t rows, int64_t cols, int64_t col0, int64_t N,
+                              int sign, int precision, void* stream);
 
 /* Device memory and stream helpers, so that callers above this ABI need no
  * CUDA runtime of their own (they replace the reference's allocBufferT /

@@ -78,10 +78,54 @@ int blocks(bool pack, const void* src, void* dst, int64_t outer, int64_t n, int 
                    : run_blocks<float2>(pack, src, dst, outer, n, nparts, s);
 }
 
+// data[k][c] *= exp(sign * 2 pi i * ((col0 + c) * k mod N) / N), a rows x cols
+// array: the twiddle between the two stages of the distributed four-step
+// FFT1D (the reference's fft1dTwiddleKernel,
+// src/cpp/fft/hipfft_method/1d/fft1d_cooley_tukey_executor.hip:57-83), here
+// with the phase reduced exactly in integers before the FP64 sincospi.
+template <typename C, typename T>
+__global__ void k_twiddle_rows(C* data, int64_t rows, int64_t cols, int64_t col0, int64_t N, int sign) {
+  const int64_t total = rows * cols;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = i / cols, c = i - k * cols;
+    const uint64_t m = ((unsigned __int128)(uint64_t)(col0 + c) * (uint64_t)k) % (uint64_t)N;
+    double s, co;
+    sincospi((double)sign * 2.0 * ((double)m / (double)N), &s, &co);
+    const C a = data[i];
+    const T cr = (T)co, sr = (T)s;
+    data[i] = C{a.x * cr - a.y * sr, a.x * sr + a.y * cr};
+  }
+}
+
+int twiddle_rows(void* data, int64_t rows, int64_t cols, int64_t col0, int64_t N, int sign,
+                 int precision, void* stream) {
+  if (!data || rows < 0 || cols < 0 || col0 < 0 || N < 1 || (sign != 1 && sign != -1) ||
+      (precision != 0 && precision != 1))
+    return report_error(SHAFFT_SM100_EINVAL, "twiddle: bad arguments");
+  const int64_t total = rows * cols;
+  if (total == 0) return 0;
+  const int64_t want = (total + 255) / 256;
+  const unsigned grid = (unsigned)(want < 148 * 16 ? want : 148 * 16);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision)
+    k_twiddle_rows<double2, double><<<grid, 256, 0, s>>>(static_cast<double2*>(data), rows, cols, col0, N, sign);
+  else
+    k_twiddle_rows<float2, float><<<grid, 256, 0, s>>>(static_cast<float2*>(data), rows, cols, col0, N, sign);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : report_error(SHAFFT_SM100_ECUDA, cudaGetErrorString(e));
+}
+
 }  // namespace
 }  // namespace shafft_sm100
 
 extern "C" {
+
+int shafft_sm100_twiddle_rows(void* data, int64_t rows, int64_t cols, int64_t col0, int64_t N,
+                              int sign, int precision, void* stream) {
+  return shafft_sm100::twiddle_rows(data, rows, cols, col0, N, sign, precision, stream);
+}
+
 
 int shafft_sm100_pack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
                              int precision, void* stream) {

@@ -1,6 +1,6 @@
 """Slab-decomposed N-D C2C transform over several GPUs (one process per GPU).
 
-This is the reference's multi-rank FFTND path for one distributed axis
+FFTND is the reference's multi-rank FFTND path for one distributed axis
 (commDims = [P, 1, ..., 1], src/cpp/slab_nd.cpp:84-254 with nda = 1), built on
 torch.distributed for the exchange (NCCL between GPUs) and on the kernel
 library for everything on the device:
@@ -22,7 +22,8 @@ buffer-swap contract (the result is in the buffer get_buffers() reports as
 data) and the (1/sqrt(N))^k normalisation.  Methods return the reference's
 status codes.  More than one distributed axis (pencils) returns
 ERR_NOT_IMPL.  Ranks beyond prod(commDims) are inactive: they own no data
-and take part in the exchanges with empty blocks.
+and take part in the exchanges with empty blocks.  FFT1D (below) is the
+reference's distributed 1-D transform (the P x P four-step path).
 """
 from __future__ import annotations
 
@@ -284,6 +285,130 @@ class FFTND:
         return 0
 
 
+class FFT1D:
+    """Distributed shafft::FFT1D over a torch.distributed group: the
+    reference's P x P four-step path (src/cpp/fft/hipfft_method/1d/
+    fft1d_cooley_tukey_executor.hip:175-290), for N divisible by P^2.  Rank r
+    holds the contiguous block x[r*L, (r+1)*L), L = N/P, before and after a
+    transform.  With C = L/P:
+
+      1. all-to-all of C-element chunks      -> [s][c] = x[s*L + r*C + c]
+      2. length-P DFTs over s (one column pass of a [P][C] plan)
+                                              -> [k1][c], already the send order
+      3. twiddle w_N^{(r*C + c) k1}           (shafft_sm100_twiddle_rows)
+      4. all-to-all                           -> [s][c] = column r*... of k1 = r
+      5. length-L DFT                         -> X[r + P*k2] at k2
+      6. all-to-all of the C-chunks of k2     -> [s][j] = X[r*L + s + P*j]
+      7. [P][C] -> [C][P] transpose           (shafft_sm100_unpack_blocks)
+
+    The result is in the buffer get_buffers() reports as data (the buffers
+    swap on every execute, Slab1D::swapBuffers).  Lengths not divisible by
+    P^2 (the reference's distributed Bluestein) return ERR_NOT_IMPL."""
+
+    def __init__(self):
+        self._state = "created"
+        self.norm_exponent = 0
+
+    def init(self, n, local_n, local_start, precision=C2C, group=None, device_ops=None) -> int:
+        import torch.distributed as dist
+        if self._state != "created":
+            return ERR_INVALID_STATE
+        if precision not in (C2C, Z2Z):
+            return ERR_INVALID_FFTTYPE
+        n, local_n, local_start = int(n), int(local_n), int(local_start)
+        if n < 1:
+            return ERR_INVALID_DIM
+        P = dist.get_world_size(group) if dist.is_initialized() else 1
+        r = dist.get_rank(group) if dist.is_initialized() else 0
+        if n % (P * P):
+            return ERR_NOT_IMPL
+        L = n // P
+        if local_n != L or local_start != r * L:
+            return ERR_INVALID_DECOMP
+        self.N, self.P, self.rank, self.L, self.C = n, P, r, L, L // P
+        self.precision, self.group, self.ops = precision, group, device_ops
+        self._state = "configured"
+        return 0
+
+    def plan(self) -> int:
+        if self._state == "created":
+            return ERR_PLAN_NOT_INIT
+        if self._state != "configured":
+            return ERR_INVALID_STATE
+        if self.ops is None:
+            self.ops = CudaOps(self.precision)
+        if self.P == 1:
+            self.plans = [self.ops.plan([self.N], [0])]
+        else:
+            self.plans = [self.ops.plan([self.P, self.C], [0]), self.ops.plan([self.L], [0])]
+        self.data = self.work = self.scratch = None
+        self._state = "planned"
+        return 0
+
+    def release(self):
+        for h in getattr(self, "plans", []):
+            self.ops.destroy(h)
+        self.plans = []
+        self._state = "released"
+
+    def alloc_size(self) -> int:
+        return self.L if self._state in ("configured", "planned") else 0
+
+    def set_buffers(self, data, work) -> int:
+        if self._state != "planned":
+            return ERR_PLAN_NOT_INIT
+        if data is None or work is None:
+            return ERR_NULLPTR
+        if data.numel() < self.L or work.numel() < self.L or data.data_ptr() == work.data_ptr():
+            return ERR_ALLOC
+        self.data, self.work = data, work
+        self.scratch = data.new_empty(self.L)  # plan-owned, as the reference's dBuf/dTemp
+        return 0
+
+    def get_buffers(self):
+        return 0, self.data, self.work
+
+    def execute(self, direction) -> int:
+        if self._state != "planned":
+            return ERR_PLAN_NOT_INIT
+        if self.data is None:
+            return ERR_NO_BUFFER
+        if direction not in (FORWARD, BACKWARD):
+            return ERR_INVALID_STATE
+        x, w, s = self.data, self.work, self.scratch
+        if self.P == 1:
+            self.ops.execute(self.plans[0], x, w, direction)
+        else:
+            P, C, L = self.P, self.C, self.L
+            eq = [C] * P
+            self.ops.alltoall(w, x, eq, eq, self.group, P)              # 1
+            self.ops.execute(self.plans[0], w, s, direction)            # 2  [k1][c]
+            self.ops.twiddle(s, P, C, self.rank * C, self.N, -1 if direction == FORWARD else 1)  # 3
+            self.ops.alltoall(x, s, eq, eq, self.group, P)              # 4
+            self.ops.execute(self.plans[1], x, s, direction)            # 5  X[r + P k2]
+            self.ops.alltoall(x, s, eq, eq, self.group, P)              # 6  [s][j]
+            self.ops.unpack(x, w, C, P, P)                              # 7  [j][s]
+        self.data, self.work = w, x
+        self.norm_exponent += 1
+        return 0
+
+    def normalize(self) -> int:
+        """(1/sqrt(N))^k, k = executes since the last normalize; the factor in
+        single precision for C2C, as the reference's fft1dNormalize."""
+        import numpy as np
+        if self._state != "planned":
+            return ERR_PLAN_NOT_INIT
+        k = self.norm_exponent
+        if k:
+            if self.precision == C2C:
+                f = float(np.float32(1.0) / np.power(np.sqrt(np.float32(self.N)), np.float32(k)))
+            else:
+                f = 1.0 / math.sqrt(self.N) ** k
+            self.ops.scale(self.data, self.L, f)
+        self.norm_exponent = 0
+        return 0
+
+
 class CudaOps:
     """Device steps of the distributed transform: kernel-library plans over
     axis subsets, block pack/unpack, scale, and the all-to-all (NCCL for CUDA
@@ -298,6 +423,9 @@ class CudaOps:
         self.lib.shafft_sm100_plan_create_axes.argtypes = [
             ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        self.lib.shafft_sm100_twiddle_rows.argtypes = [
+            ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+            ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         for f in (self.lib.shafft_sm100_pack_blocks, self.lib.shafft_sm100_unpack_blocks):
             f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                           ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
@@ -332,6 +460,10 @@ class CudaOps:
     def unpack(self, src, dst, outer, n, P):
         self._sm._check(self.lib.shafft_sm100_unpack_blocks(src.data_ptr(), dst.data_ptr(), outer, n, P,
                                                             self.precision, self._stream()), "unpack")
+
+    def twiddle(self, data, rows, cols, col0, n, sign):
+        self._sm._check(self.lib.shafft_sm100_twiddle_rows(data.data_ptr(), rows, cols, col0, n, sign,
+                                                           self.precision, self._stream()), "twiddle")
 
     def scale(self, data, count, factor):
         self._sm._check(self.lib.shafft_sm100_scale(ctypes.c_void_p(data.data_ptr()), count,

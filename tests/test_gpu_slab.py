@@ -142,3 +142,61 @@ def test_distributed_fftnd_two_ranks(tmp_path, dims, prec, policy):
         assert sum(x["fwd_layout"][0][-1] for x in res) == dims[-1]
     else:
         assert sum(x["fwd_layout"][0][0] for x in res) == dims[0]
+
+
+WORKER_1D = r'''
+import json, math, sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np, torch, torch.distributed as dist
+import shafft_b200 as S
+from shafft_b200 import slab
+from oracle import oracle as o
+cfg = json.loads(sys.argv[3])
+torch.cuda.set_device(0)
+dist.init_process_group("gloo")
+r, P = dist.get_rank(), dist.get_world_size()
+N, prec = cfg["n"], cfg["prec"]
+L = N // P
+dt = np.complex128 if prec == S.Z2Z else np.complex64
+g = o.uniform_input((N,), seed=42, dtype=dt)
+ref = o.fftn(g.astype(np.complex128), precise=(prec == S.Z2Z))[r * L:(r + 1) * L]
+plan = slab.FFT1D()
+assert plan.init(N, L, r * L, prec) == 0
+assert plan.plan() == 0
+tdt = torch.complex128 if prec == S.Z2Z else torch.complex64
+a = torch.zeros(L, dtype=tdt, device="cuda"); b = torch.zeros_like(a)
+assert plan.set_buffers(a, b) == 0
+a.copy_(torch.from_numpy(g[r * L:(r + 1) * L]).cuda())
+assert plan.execute(S.FORWARD) == 0
+_, d, _ = plan.get_buffers()
+y = d.cpu().numpy()
+err2 = float(np.sum(np.abs(y - ref) ** 2)); ref2 = float(np.sum(np.abs(ref) ** 2))
+assert plan.execute(S.BACKWARD) == 0 and plan.normalize() == 0
+_, d, _ = plan.get_buffers()
+x = g[r * L:(r + 1) * L]
+bt2 = float(np.sum(np.abs(d.cpu().numpy() - x) ** 2)); g2 = float(np.sum(np.abs(x) ** 2))
+plan.release()
+dist.destroy_process_group()
+json.dump({"err2": err2, "ref2": ref2, "bt2": bt2, "g2": g2}, open(sys.argv[2], "w"))
+'''
+
+
+@pytest.mark.parametrize("n,prec", [(1 << 20, S.C2C), (121500, S.C2C), (1 << 18, S.Z2Z)])
+def test_distributed_fft1d_two_ranks(tmp_path, n, prec):
+    world = 2
+    script = tmp_path / "worker1d.py"
+    script.write_text(WORKER_1D)
+    port = _free_port()
+    procs = []
+    for r in range(world):
+        env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
+                   RANK=str(r), LOCAL_RANK=str(r))
+        procs.append(subprocess.Popen([sys.executable, str(script), ROOT, str(tmp_path / f"r{r}.json"),
+                                       json.dumps({"n": n, "prec": prec})], env=env))
+    for p in procs:
+        assert p.wait(timeout=300) == 0
+    res = [json.loads((tmp_path / f"r{r}.json").read_text()) for r in range(world)]
+    err = math.sqrt(sum(x["err2"] for x in res) / sum(x["ref2"] for x in res))
+    back = math.sqrt(sum(x["bt2"] for x in res) / sum(x["g2"] for x in res))
+    assert err <= tol(n, prec), err
+    assert back <= 2 * tol(n, prec), back

@@ -50,6 +50,11 @@ class NumpyOps:
             out[:, s:s + l] = src[pos:pos + outer * l].numpy().reshape(outer, l); pos += outer * l
         dst[:outer * n] = torch.from_numpy(out.ravel())
     def scale(self, data, count, f): data[:count] *= f
+    def twiddle(self, data, rows, cols, col0, n, sign):
+        k = np.arange(rows)[:, None]; c = np.arange(cols)[None, :]
+        m = ((col0 + c) * k) % n
+        w = np.exp(sign * 2j * np.pi * m / n).ravel()
+        data[:rows * cols] *= torch.from_numpy(w)
     def alltoall(self, out, inp, oc, ic, group, world):
         o = torch.view_as_real(out[:sum(oc)]).view(-1); i = torch.view_as_real(inp[:sum(ic)]).view(-1)
         dist.all_to_all_single(o, i, [2 * c for c in oc], [2 * c for c in ic], group=group)
@@ -57,6 +62,29 @@ class NumpyOps:
 cfg = json.loads(sys.argv[3])
 dist.init_process_group("gloo")
 rank, world = dist.get_rank(), dist.get_world_size()
+if cfg.get("fft1d"):
+    N = cfg["n"]; L = N // world
+    rng = np.random.Generator(np.random.MT19937(9))
+    g = rng.uniform(-1, 1, N) + 1j * rng.uniform(-1, 1, N)
+    plan = slab.FFT1D()
+    rc = plan.init(N, L, rank * L, S.Z2Z, None, device_ops=NumpyOps())
+    out = {"rank": rank, "init": rc}
+    if rc == 0:
+        assert plan.plan() == 0
+        a = torch.zeros(L, dtype=torch.complex128); b = torch.zeros_like(a)
+        assert plan.set_buffers(a, b) == 0
+        _, d, _ = plan.get_buffers(); d[:] = torch.from_numpy(g[rank * L:(rank + 1) * L])
+        assert plan.execute(S.FORWARD) == 0
+        _, d2, _ = plan.get_buffers()
+        out["swapped"] = d2.data_ptr() != d.data_ptr()
+        ref = np.fft.fft(g)[rank * L:(rank + 1) * L]
+        out["fwd_err"] = float(np.abs(d2.numpy() - ref).max() / np.abs(ref).max())
+        assert plan.execute(S.BACKWARD) == 0 and plan.normalize() == 0
+        _, d3, _ = plan.get_buffers()
+        out["rt_err"] = float(np.abs(d3.numpy() - g[rank * L:(rank + 1) * L]).max())
+    dist.destroy_process_group()
+    json.dump(out, open(sys.argv[2], "w"))
+    sys.exit(0)
 dims = tuple(cfg["dims"]); P = cfg["P"]
 rng = np.random.Generator(np.random.MT19937(5))
 g = rng.uniform(-1, 1, dims) + 1j * rng.uniform(-1, 1, dims)
@@ -149,3 +177,19 @@ def test_init_validation():
     assert p.init([2, 1], [8, 8]) == S.ERR_INVALID_DECOMP       # 2 parts, 1 process
     p = slab.FFTND()
     assert p.plan() == S.ERR_PLAN_NOT_INIT
+
+
+@pytest.mark.parametrize("world,n", [(2, 64), (3, 9 * 7), (2, 4 * 1000), (4, 16 * 5)])
+def test_slab_fft1d_four_step_on_gloo_ranks(tmp_path, world, n):
+    res = _run(tmp_path, world, {"fft1d": True, "n": n})
+    for o in res:
+        assert o["init"] == 0
+        assert o["swapped"]
+        assert o["fwd_err"] < 1e-12, o
+        assert o["rt_err"] < 1e-12, o
+
+
+def test_slab_fft1d_needs_p_squared(tmp_path):
+    import shafft_b200 as S
+    res = _run(tmp_path, 2, {"fft1d": True, "n": 6})   # 6 % 4 != 0
+    assert all(o["init"] == S.ERR_NOT_IMPL for o in res)
