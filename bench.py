@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--tensor-core", action="store_true",
                     help="plan with the tensor-core form (complex64; debug / profiling of that form)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-lanes", type=int, default=2,
+                    help="plans / host threads of the e2e arm (overlapping steps)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--suite", default="headline", choices=["headline", "batched", "serve", "configs", "tc"],
                     help="headline (default, the contract line) or one of the side workloads")
@@ -401,7 +403,7 @@ def e2e_arm(S, dims, n, args, stream, barrier, dist):
     import threading
 
     import torch
-    lanes = 2
+    lanes = max(1, args.e2e_lanes)
     lib = S.load()
     nbytes = 8 * n
     plans, bufs, hosts = [], [], []
@@ -465,8 +467,8 @@ def e2e_arm(S, dims, n, args, stream, barrier, dist):
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": k,
             "ms_per_step": tmax / k,
             "path": "libshafft.so C ABI: shafftCopyToBufferF, shafftExecuteNormalized x2, "
-                    "shafftCopyFromBufferF, pinned host buffers; 2 plans on 2 host threads "
-                    "(steps overlap), host wall clock between barriers"}
+                    f"shafftCopyFromBufferF, pinned host buffers; {lanes} plans on {lanes} host "
+                    "threads (steps overlap), host wall clock between barriers"}
 
 
 # ---------------------------------------------------------------------------
