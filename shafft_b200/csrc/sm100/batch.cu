@@ -75,8 +75,10 @@ bool smooth13(int64_t L) {
   return L == 1;
 }
 
+// complex64: at most 80 registers so that three CTAs share an SM (the tiles
+// are latency-bound; 116 registers allowed only two); complex128 unbounded
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1)
     k_fft_batch(const SlotDesc<typename Cx<T>::type>* slots, const int64_t* start, int nslots,
                 typename Cx<T>::type* const* src, typename Cx<T>::type* const* dst, int* done,
                 unsigned long long* ticket, int* err, int conj, double scale) {
