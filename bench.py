@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--dims", default=None, help="override the 512^3 workload (debug only)")
     ap.add_argument("--tensor-core", action="store_true",
                     help="plan with the tensor-core form (complex64; debug / profiling of that form)")
+    ap.add_argument("--plan-flags", type=int, default=0,
+                    help="SHAFFT_SM100_PLAN_* flags of the plan (debug / profiling; 2 = tensor cores "
+                         "on prime-factor axes)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-lanes", type=int, default=2,
                     help="plans / host threads of the e2e arm (overlapping steps)")
@@ -290,7 +293,7 @@ def ours(args):
 
     dims = tuple(int(v) for v in args.dims.split("x")) if args.dims else DIMS
     n = math.prod(dims)
-    plan = _sm100.Plan(dims, 0, _sm100.PLAN_TENSOR_CORE if args.tensor_core else 0)
+    plan = _sm100.Plan(dims, 0, (_sm100.PLAN_TENSOR_CORE if args.tensor_core else 0) | args.plan_flags)
     nst = plan.launches
     scale = float(1.0 / math.sqrt(n))
     # a dedicated stream: the kernels and the events that time them share it
