@@ -65,6 +65,16 @@ int shafft_sm100_plan_create_nd(shafft_sm100_plan* out, int ndim, const int64_t*
  * plain specialised passes.  Ignored when SHAFFT_SM100_PLAN_TENSOR_CORE is
  * also set.  No counterpart in the reference. */
 #define SHAFFT_SM100_PLAN_TC_PRIME_AXES 2
+/* SHAFFT_SM100_PLAN_MEASURE (or SHAFFT_SM100_PLANNER=MEASURE in the
+ * environment, which applies it to every plan): build and time each distinct
+ * pass list the planner's choices give for this shape (multi-pass factor
+ * splits, generic tile widths, and -- only with
+ * SHAFFT_SM100_PLAN_TC_PRIME_AXES -- tensor-core passes or not), keep the
+ * fastest, and cache the choice per shape in SHAFFT_SM100_PLAN_CACHE (default
+ * ~/.cache/shafft_sm100_plans.txt).  Plan creation then allocates two
+ * transform-sized scratch buffers for the duration of the measurement.  The
+ * counterpart of the reference's SHAFFT_FFTW_PLANNER=MEASURE. */
+#define SHAFFT_SM100_PLAN_MEASURE 4
 
 int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64_t* dims,
                                    int precision, int flags);

@@ -88,6 +88,7 @@ def _check(rc, what):
 # plan flags (shafft_sm100.h)
 PLAN_TENSOR_CORE = 1
 PLAN_TC_PRIME_AXES = 2
+PLAN_MEASURE = 4
 
 
 def plan_query(dims, precision=0, flags=0) -> dict:

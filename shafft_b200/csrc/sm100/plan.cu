@@ -28,6 +28,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
 
 #include <algorithm>
 #include <functional>
@@ -166,6 +167,13 @@ struct Planner {
   size_t table_bytes = 0;
   int64_t scratch_elems = 0;
 
+  // Planning choices that measurements decide (SHAFFT_SM100_PLAN_MEASURE
+  // times them per shape; the defaults are the measured-best rules):
+  //   balanced  multi-pass splits as balanced as possible (default for
+  //             complex64) instead of the largest last factor
+  //   widen     narrower generic tiles for passes with few tiles
+  int balanced = -1;  // -1: by precision
+  int widen = 1;
   // tensor-core planning: every pass of length <= 64 is a tcgen05 pass
   int tc_mode = 0;
   bool cur_tc = false;  // set while the passes being built are tensor-core passes
@@ -224,7 +232,7 @@ struct Planner {
   // passes that already have a few hundred tiles lose from narrower tiles
   // (105^3, 1,488,375), so they are left alone.
   void widen_grid(Step& st) {
-    if (st.fast || st.tc || st.kind != ST_PASS) return;
+    if (!widen || st.fast || st.tc || st.kind != ST_PASS) return;
     const int64_t want = 2 * 148;
     while (st.g.W > 2 && st.g.ntiles < want) finish_geom(st, st.g.W / 2);
   }
@@ -433,7 +441,7 @@ struct Planner {
         const int64_t c = L / d;
         // complex128 (tiles twice the bytes): the largest last factor wins
         // instead (2^24 = 64*512*512: 0.78 ms vs 0.87 ms for 256^3)
-        const bool first_only = precision != 0;
+        const bool first_only = balanced < 0 ? precision != 0 : balanced == 0;
         if (fast_len(c) && c >= 16 && std::min(c, d) > m2 && !(first_only && m2 > 0)) {
           m2 = std::min(c, d);
           best2 = {(int)c, (int)d};
@@ -462,6 +470,7 @@ struct Planner {
         if (c < 2 || c > lim.max_col || std::min(c, d) <= bm) continue;
         bm = std::min(c, d);
         best = {(int)c, (int)d};
+        if (balanced == 0) break;  // the largest last factor that fits
       }
     }
     if (!best.empty()) return best;
@@ -1122,9 +1131,222 @@ int axes_mask(int ndim, int naxes, const int* axes, uint64_t* mask) {
   return 0;
 }
 
+// ---- plan creation with explicit planning choices ------------------------
+
+struct Knobs {
+  int balanced = -1;  // -1: by precision
+  int widen = 1;
+  int tc = -1;        // -1: as the flags say; 0: plain; 2: tensor cores on prime-factor axes
+};
+
+int effective_flags(int flags, const Knobs& k) {
+  if (k.tc == 0) flags &= ~(SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES);
+  if (k.tc == 2) flags = (flags & ~SHAFFT_SM100_PLAN_TENSOR_CORE) | SHAFFT_SM100_PLAN_TC_PRIME_AXES;
+  return flags;
+}
+
+void configure(Planner& pl, const Knobs& k, uint64_t mask) {
+  pl.axes_mask = mask;
+  pl.balanced = k.balanced;
+  pl.widen = k.widen;
+}
+
+int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int precision, int flags,
+                uint64_t mask, int64_t total, const Knobs& k) {
+  flags = effective_flags(flags, k);
+  std::unique_ptr<shafft_sm100_plan_s> p(new (std::nothrow) shafft_sm100_plan_s());
+  if (!p) return set_err(SHAFFT_SM100_EALLOC, "host allocation failed");
+  p->precision = precision;
+  p->ndim = ndim;
+  p->dims.assign(dims, dims + ndim);
+  p->total = total;
+  p->flags = flags;
+  Planner pl(precision, flags);
+  configure(pl, k, mask);
+  int rc = pl.plan_nd(p->steps, ndim, dims);
+  if (rc) return rc;
+  p->off_tcerr = pl.off_tcerr;
+  p->ltabs = pl.ltabs;
+  p->ntabs = pl.ntabs;
+  p->btabs = pl.btabs;
+  p->table_bytes = std::max<size_t>(pl.table_bytes, 256);
+  p->scratch_elems = pl.scratch_elems;
+  CUDA_TRY(cudaGetDevice(&p->device));
+  if (cudaMalloc(&p->d_tables, p->table_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for tables failed", p->table_bytes);
+  }
+  if (p->scratch_elems > 0) {
+    const size_t b = (size_t)p->scratch_elems * (precision ? 16 : 8);
+    if (cudaMalloc(&p->d_s0, b) != cudaSuccess || cudaMalloc(&p->d_s1, b) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(p->d_tables);
+      if (p->d_s0) cudaFree(p->d_s0);
+      return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for scratch failed", b);
+    }
+  }
+  if (cudaMemset(p->d_tables, 0, p->table_bytes) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(p->d_tables);
+    if (p->d_s0) cudaFree(p->d_s0);
+    if (p->d_s1) cudaFree(p->d_s1);
+    return set_err(SHAFFT_SM100_ECUDA, "cudaMemset of the plan tables failed");
+  }
+  rc = precision ? Launcher<double>::build_tables(p.get()) : Launcher<float>::build_tables(p.get());
+  if (rc) {
+    cudaFree(p->d_tables);
+    if (p->d_s0) cudaFree(p->d_s0);
+    if (p->d_s1) cudaFree(p->d_s1);
+    return rc;
+  }
+  *out = p.release();
+  return 0;
+}
+
+// ---- measured planning (SHAFFT_SM100_PLAN_MEASURE) ------------------------
+//
+// The analogue of the reference's FFTW planner effort (SHAFFT_FFTW_PLANNER=
+// MEASURE, src/cpp/fft/fftw_method/common/env.hpp:29-46): every distinct pass
+// list the planning choices yield is built and timed (forward transforms of
+// zeros on two scratch buffers, 2 warm-up + 5 timed, CUDA events), the
+// fastest choice is kept and cached per shape in the text file
+// SHAFFT_SM100_PLAN_CACHE (default ~/.cache/shafft_sm100_plans.txt).  The
+// tensor-core alternative is only considered when the caller allowed it
+// with SHAFFT_SM100_PLAN_TC_PRIME_AXES.  If the scratch buffers cannot be
+// allocated the default choices are used.
+
+std::mutex g_plan_cache_mu;
+
+std::string plan_cache_path() {
+  if (const char* e = getenv("SHAFFT_SM100_PLAN_CACHE")) return e;
+  const char* home = getenv("HOME");
+  return std::string(home ? home : ".") + "/.cache/shafft_sm100_plans.txt";
+}
+
+std::string plan_key(int ndim, const int64_t* dims, int precision, int flags, uint64_t mask) {
+  std::string k = (precision ? "c128" : "c64") + std::string(":f") + std::to_string(flags) + ":m" +
+                  std::to_string((unsigned long long)mask) + ":";
+  for (int a = 0; a < ndim; ++a) k += (a ? "x" : "") + std::to_string((long long)dims[a]);
+  return k;
+}
+
+bool cache_lookup(const std::string& key, Knobs* k) {
+  std::lock_guard<std::mutex> lk(g_plan_cache_mu);
+  FILE* f = fopen(plan_cache_path().c_str(), "r");
+  if (!f) return false;
+  char line[1024];
+  bool found = false;
+  while (fgets(line, sizeof(line), f)) {
+    char name[900];
+    Knobs t;
+    if (sscanf(line, "%899s %d %d %d", name, &t.balanced, &t.widen, &t.tc) == 4 && key == name) {
+      *k = t;  // the last entry of a key wins
+      found = true;
+    }
+  }
+  fclose(f);
+  return found;
+}
+
+void cache_store(const std::string& key, const Knobs& k) {
+  std::lock_guard<std::mutex> lk(g_plan_cache_mu);
+  const std::string path = plan_cache_path();
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {
+    const std::string dir = path.substr(0, slash);
+    mkdir(dir.c_str(), 0755);  // best effort; an existing directory is fine
+  }
+  if (FILE* f = fopen(path.c_str(), "a")) {
+    fprintf(f, "%s %d %d %d\n", key.c_str(), k.balanced, k.widen, k.tc);
+    fclose(f);
+  }
+}
+
+// forward time of a plan in ms (negative on failure)
+double time_forward(shafft_sm100_plan p, void* a, void* b) {
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double ms = -1.0;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
+      cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; ++i) ok = shafft_sm100_execute(p, a, b, 0, 1.0, s) == 0;
+    cudaEventRecord(e0, s);
+    for (int i = 0; i < 5 && ok; ++i) ok = shafft_sm100_execute(p, a, b, 0, 1.0, s) == 0;
+    cudaEventRecord(e1, s);
+    float t = 0;
+    if (ok && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess &&
+        shafft_sm100_plan_status(p) == 0)
+      ms = t / 5.0;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  cudaGetLastError();
+  return ms;
+}
+
+Knobs measured_knobs(int ndim, const int64_t* dims, int precision, int flags, uint64_t mask,
+                     int64_t total) {
+  const std::string key = plan_key(ndim, dims, precision, flags, mask);
+  Knobs best;
+  if (cache_lookup(key, &best)) return best;
+  std::vector<Knobs> cands;
+  const bool tc_alt = precision == 0 && (flags & SHAFFT_SM100_PLAN_TC_PRIME_AXES) &&
+                      !(flags & SHAFFT_SM100_PLAN_TENSOR_CORE);
+  for (int bal : {1, 0})
+    for (int wid : {1, 0})
+      for (int tc : tc_alt ? std::vector<int>{0, 2} : std::vector<int>{-1}) {
+        Knobs k;
+        k.balanced = bal;
+        k.widen = wid;
+        k.tc = tc;
+        cands.push_back(k);
+      }
+  // keep one candidate per distinct pass list
+  std::vector<Knobs> distinct;
+  std::vector<std::string> seen;
+  for (const Knobs& k : cands) {
+    Planner pl(precision, effective_flags(flags, k));
+    configure(pl, k, mask);
+    std::vector<Step> steps;
+    if (pl.plan_nd(steps, ndim, dims)) continue;
+    const std::string d = describe_steps(precision, steps, total);
+    if (std::find(seen.begin(), seen.end(), d) != seen.end()) continue;
+    seen.push_back(d);
+    distinct.push_back(k);
+  }
+  if (distinct.size() <= 1) return distinct.empty() ? Knobs{} : distinct[0];
+  const size_t bytes = (size_t)total * (precision ? 16 : 8);
+  void *a = nullptr, *b = nullptr;
+  if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    if (a) cudaFree(a);
+    return Knobs{};
+  }
+  cudaMemset(a, 0, bytes);
+  double best_ms = -1.0;
+  best = distinct[0];
+  for (const Knobs& k : distinct) {
+    shafft_sm100_plan p = nullptr;
+    if (create_plan(&p, ndim, dims, precision, flags, mask, total, k)) continue;
+    const double ms = time_forward(p, a, b);
+    shafft_sm100_plan_destroy(p);
+    if (ms >= 0 && (best_ms < 0 || ms < best_ms)) {
+      best_ms = ms;
+      best = k;
+    }
+  }
+  cudaFree(a);
+  cudaFree(b);
+  if (best_ms >= 0) cache_store(key, best);
+  return best;
+}
+
 int validate_flags(int flags, int precision) {
   const int tc_flags = SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES;
-  if (flags & ~tc_flags) return set_err(SHAFFT_SM100_EINVAL, "unknown plan flags");
+  if (flags & ~(tc_flags | SHAFFT_SM100_PLAN_MEASURE))
+    return set_err(SHAFFT_SM100_EINVAL, "unknown plan flags");
   if ((flags & tc_flags) && precision != 0)
     return set_err(SHAFFT_SM100_ENOTSUP, "the tensor-core form is complex64 only");
   return 0;
@@ -1166,8 +1388,15 @@ int shafft_sm100_plan_query_axes(int ndim, const int64_t* dims, int precision, i
   uint64_t mask = 0;
   rc = axes_mask(ndim, naxes, axes, &mask);
   if (rc) return rc;
+  // a measured plan is described with its cached choice (no measuring here)
+  const char* env = getenv("SHAFFT_SM100_PLANNER");
+  const bool measure = (flags & SHAFFT_SM100_PLAN_MEASURE) || (env && strcmp(env, "MEASURE") == 0);
+  flags &= ~SHAFFT_SM100_PLAN_MEASURE;
+  Knobs k;
+  if (measure) cache_lookup(plan_key(ndim, dims, precision, flags, mask), &k);
+  flags = effective_flags(flags, k);
   Planner pl(precision, flags);
-  pl.axes_mask = mask;
+  configure(pl, k, mask);
   std::vector<Step> steps;
   rc = pl.plan_nd(steps, ndim, dims);
   if (rc) return rc;
@@ -1195,53 +1424,12 @@ int shafft_sm100_plan_create_axes(shafft_sm100_plan* out, int ndim, const int64_
   uint64_t mask = 0;
   rc = axes_mask(ndim, naxes, axes, &mask);
   if (rc) return rc;
-  std::unique_ptr<shafft_sm100_plan_s> p(new (std::nothrow) shafft_sm100_plan_s());
-  if (!p) return set_err(SHAFFT_SM100_EALLOC, "host allocation failed");
-  p->precision = precision;
-  p->ndim = ndim;
-  p->dims.assign(dims, dims + ndim);
-  p->total = total;
-  p->flags = flags;
-  Planner pl(precision, flags);
-  pl.axes_mask = mask;
-  rc = pl.plan_nd(p->steps, ndim, dims);
-  if (rc) return rc;
-  p->off_tcerr = pl.off_tcerr;
-  p->ltabs = pl.ltabs;
-  p->ntabs = pl.ntabs;
-  p->btabs = pl.btabs;
-  p->table_bytes = std::max<size_t>(pl.table_bytes, 256);
-  p->scratch_elems = pl.scratch_elems;
-  CUDA_TRY(cudaGetDevice(&p->device));
-  if (cudaMalloc(&p->d_tables, p->table_bytes) != cudaSuccess) {
-    cudaGetLastError();
-    return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for tables failed", p->table_bytes);
-  }
-  if (p->scratch_elems > 0) {
-    const size_t b = (size_t)p->scratch_elems * (precision ? 16 : 8);
-    if (cudaMalloc(&p->d_s0, b) != cudaSuccess || cudaMalloc(&p->d_s1, b) != cudaSuccess) {
-      cudaGetLastError();
-      cudaFree(p->d_tables);
-      if (p->d_s0) cudaFree(p->d_s0);
-      return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for scratch failed", b);
-    }
-  }
-  if (cudaMemset(p->d_tables, 0, p->table_bytes) != cudaSuccess) {
-    cudaGetLastError();
-    cudaFree(p->d_tables);
-    if (p->d_s0) cudaFree(p->d_s0);
-    if (p->d_s1) cudaFree(p->d_s1);
-    return set_err(SHAFFT_SM100_ECUDA, "cudaMemset of the plan tables failed");
-  }
-  rc = precision ? Launcher<double>::build_tables(p.get()) : Launcher<float>::build_tables(p.get());
-  if (rc) {
-    cudaFree(p->d_tables);
-    if (p->d_s0) cudaFree(p->d_s0);
-    if (p->d_s1) cudaFree(p->d_s1);
-    return rc;
-  }
-  *out = p.release();
-  return 0;
+  const char* env = getenv("SHAFFT_SM100_PLANNER");
+  const bool measure = (flags & SHAFFT_SM100_PLAN_MEASURE) || (env && strcmp(env, "MEASURE") == 0);
+  flags &= ~SHAFFT_SM100_PLAN_MEASURE;
+  Knobs k;
+  if (measure) k = measured_knobs(ndim, dims, precision, flags, mask, total);
+  return create_plan(out, ndim, dims, precision, flags, mask, total, k);
 }
 
 int shafft_sm100_plan_create_1d(shafft_sm100_plan* out, int64_t n, int precision) {

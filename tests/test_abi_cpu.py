@@ -203,4 +203,19 @@ def test_planner_tensor_core_modes():
         with pytest.raises(_sm100.Sm100Error):
             _sm100.plan_query([64], bad_prec, flags)
     with pytest.raises(_sm100.Sm100Error):
-        _sm100.plan_query([64], 0, 4)
+        _sm100.plan_query([64], 0, 8)
+
+
+def test_measured_plan_query_uses_cached_choice(tmp_path, monkeypatch):
+    """A measured plan's host-only description follows the per-shape cache
+    (written by plan creation on a GPU); without an entry it is the default."""
+    cache = tmp_path / "plans.txt"
+    monkeypatch.setenv("SHAFFT_SM100_PLAN_CACHE", str(cache))
+    M = _sm100.PLAN_MEASURE
+    lens = lambda q: [s["L"] for s in q["steps"] if s["kind"] == "pass"]
+    assert lens(_sm100.plan_query([1 << 24], 0, M)) == [256, 256, 256]
+    # key: precision, flags without the measure bit, axis mask, dims; then
+    # balanced, widen, tensor-core choice
+    cache.write_text("c64:f0:m18446744073709551615:16777216 0 1 -1\n")
+    assert lens(_sm100.plan_query([1 << 24], 0, M)) == [16, 1024, 1024]
+    assert lens(_sm100.plan_query([1 << 24], 0)) == [256, 256, 256]
