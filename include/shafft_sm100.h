@@ -195,17 +195,18 @@ int shafft_sm100_server_reset_stats(shafft_sm100_server s);
 int shafft_sm100_server_destroy(shafft_sm100_server s);
 
 /* ---- Slab exchange helpers (distributed N-D transforms) -----------------
- * src / dst: device arrays, viewed as [outer][n] row-major complex elements.
- * pack: dst = the nparts column blocks of src one after the other, block p =
- * columns [start_p, start_p + len_p) of every row as an [outer][len_p]
- * array, (len_p, start_p) the block partition of n (the first n % nparts
- * blocks one element longer); unpack is the inverse.  Asynchronous on
- * `stream`.  Replaces the subarray datatypes of the reference's
- * MPI_Alltoallw exchange (src/cpp/slab_nd.cpp:23-56). */
-int shafft_sm100_pack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
-                             int precision, void* stream);
-int shafft_sm100_unpack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
-                               int precision, void* stream);
+ * src / dst: device arrays, viewed as [outer][n][inner] row-major complex
+ * elements (n = the axis being redistributed).  pack: dst = the nparts
+ * blocks of that axis one after the other, block p = indices [start_p,
+ * start_p + len_p) as an [outer][len_p][inner] array, (len_p, start_p) the
+ * block partition of n (the first n % nparts blocks one element longer);
+ * unpack is the inverse.  Asynchronous on `stream`.  Replaces the subarray
+ * datatypes of the reference's MPI_Alltoallw exchange
+ * (src/cpp/slab_nd.cpp:23-56). */
+int shafft_sm100_pack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int64_t inner,
+                             int nparts, int precision, void* stream);
+int shafft_sm100_unpack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int64_t inner,
+                               int nparts, int precision, void* stream);
 /* data[k][c] *= exp(sign * 2*pi*i * ((col0 + c) * k mod N) / N) over a
  * rows x cols array (phase reduced in integers, FP64 sincospi): the twiddle
  * between the stages of the distributed four-step FFT1D (replaces the

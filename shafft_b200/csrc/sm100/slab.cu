@@ -1,13 +1,14 @@
-// Block packing for the slab exchange of a distributed N-D transform.
+// Block packing for the slab / pencil exchanges of a distributed N-D transform.
 //
-// A rank holding a row-major array [outer][n] (n = the last axis) sends peer
-// p the columns [start_p, start_p + len_p) of every row, where (len_p,
-// start_p) is the block partition of n over P parts: the first n % P parts
-// get one extra element (the reference's block_partition,
-// src/cpp/detail/partition.hpp:40-44).  pack writes the P blocks one after
-// the other, each [outer][len_p] row-major, so that block p is one
-// contiguous segment of an all-to-all send buffer; unpack is the inverse.
-// Blocks received along the leading axis need neither: they are row ranges.
+// A rank holding a row-major array [outer][n][inner] (n = the axis being
+// redistributed) sends peer p the index range [start_p, start_p + len_p) of
+// that axis, where (len_p, start_p) is the block partition of n over P parts:
+// the first n % P parts get one extra element (the reference's
+// block_partition, src/cpp/detail/partition.hpp:40-44).  pack writes the P
+// blocks one after the other, each [outer][len_p][inner] row-major, so that
+// block p is one contiguous segment of an all-to-all send buffer; unpack is
+// the inverse.  Blocks along the outermost axis (outer == 1) are already
+// contiguous and need neither.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -35,16 +36,19 @@ struct BlockMap {
   }
 };
 
-// one thread per element of the [outer][n] array; pack: array -> blocks
+// one thread per element of the [outer][n][inner] array; pack: array -> blocks
 template <typename C, bool PACK>
-__global__ void k_blocks(const C* __restrict__ src, C* __restrict__ dst, int64_t outer, BlockMap bm) {
-  const int64_t total = outer * bm.n;
+__global__ void k_blocks(const C* __restrict__ src, C* __restrict__ dst, int64_t outer, int64_t inner,
+                         BlockMap bm) {
+  const int64_t row_len = bm.n * inner;
+  const int64_t total = outer * row_len;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = i / bm.n, k = i - row * bm.n;
+    const int64_t row = i / row_len, rem = i - row * row_len;
+    const int64_t k = rem / inner, ii = rem - k * inner;
     int64_t start, len;
     bm.locate(k, start, len);
-    const int64_t b = outer * start + row * len + (k - start);
+    const int64_t b = (outer * start + row * len + (k - start)) * inner + ii;
     if (PACK)
       dst[b] = src[i];
     else
@@ -53,29 +57,29 @@ __global__ void k_blocks(const C* __restrict__ src, C* __restrict__ dst, int64_t
 }
 
 template <typename C>
-int run_blocks(bool pack, const void* src, void* dst, int64_t outer, int64_t n, int nparts,
-               cudaStream_t s) {
+int run_blocks(bool pack, const void* src, void* dst, int64_t outer, int64_t n, int64_t inner,
+               int nparts, cudaStream_t s) {
   BlockMap bm{n, n / nparts, n % nparts};
-  const int64_t total = outer * n;
+  const int64_t total = outer * n * inner;
   if (total == 0) return 0;
   const int64_t want = (total + 255) / 256;
   const unsigned grid = (unsigned)(want < 148 * 16 ? want : 148 * 16);
   if (pack)
-    k_blocks<C, true><<<grid, 256, 0, s>>>(static_cast<const C*>(src), static_cast<C*>(dst), outer, bm);
+    k_blocks<C, true><<<grid, 256, 0, s>>>(static_cast<const C*>(src), static_cast<C*>(dst), outer, inner, bm);
   else
-    k_blocks<C, false><<<grid, 256, 0, s>>>(static_cast<const C*>(src), static_cast<C*>(dst), outer, bm);
+    k_blocks<C, false><<<grid, 256, 0, s>>>(static_cast<const C*>(src), static_cast<C*>(dst), outer, inner, bm);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? 0 : report_error(SHAFFT_SM100_ECUDA, cudaGetErrorString(e));
 }
 
-int blocks(bool pack, const void* src, void* dst, int64_t outer, int64_t n, int nparts, int precision,
-           void* stream) {
+int blocks(bool pack, const void* src, void* dst, int64_t outer, int64_t n, int64_t inner, int nparts,
+           int precision, void* stream) {
   if (!src || !dst || src == dst) return report_error(SHAFFT_SM100_EINVAL, "block pack: bad buffers");
-  if (outer < 0 || n < 1 || nparts < 1 || nparts > n || (precision != 0 && precision != 1))
+  if (outer < 0 || inner < 1 || n < 1 || nparts < 1 || nparts > n || (precision != 0 && precision != 1))
     return report_error(SHAFFT_SM100_EINVAL, "block pack: bad sizes");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  return precision ? run_blocks<double2>(pack, src, dst, outer, n, nparts, s)
-                   : run_blocks<float2>(pack, src, dst, outer, n, nparts, s);
+  return precision ? run_blocks<double2>(pack, src, dst, outer, n, inner, nparts, s)
+                   : run_blocks<float2>(pack, src, dst, outer, n, inner, nparts, s);
 }
 
 // data[k][c] *= exp(sign * 2 pi i * ((col0 + c) * k mod N) / N), a rows x cols
@@ -127,14 +131,14 @@ int shafft_sm100_twiddle_rows(void* data, int64_t rows, int64_t cols, int64_t co
 }
 
 
-int shafft_sm100_pack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
-                             int precision, void* stream) {
-  return shafft_sm100::blocks(true, src, dst, outer, n, nparts, precision, stream);
+int shafft_sm100_pack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int64_t inner,
+                             int nparts, int precision, void* stream) {
+  return shafft_sm100::blocks(true, src, dst, outer, n, inner, nparts, precision, stream);
 }
 
-int shafft_sm100_unpack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int nparts,
-                               int precision, void* stream) {
-  return shafft_sm100::blocks(false, src, dst, outer, n, nparts, precision, stream);
+int shafft_sm100_unpack_blocks(const void* src, void* dst, int64_t outer, int64_t n, int64_t inner,
+                               int nparts, int precision, void* stream) {
+  return shafft_sm100::blocks(false, src, dst, outer, n, inner, nparts, precision, stream);
 }
 
 }  // extern "C"

@@ -1,33 +1,37 @@
-"""Slab-decomposed N-D C2C transform over several GPUs (one process per GPU).
+"""Distributed C2C transforms over several GPUs (one process per GPU).
 
-FFTND is the reference's multi-rank FFTND path for one distributed axis
-(commDims = [P, 1, ..., 1], src/cpp/slab_nd.cpp:84-254 with nda = 1), built on
-torch.distributed for the exchange (NCCL between GPUs) and on the kernel
-library for everything on the device:
+FFTND is the reference's multi-rank FFTND: commDims = [P_0, ..., P_{nda-1},
+1, ..., 1] distributes the leading nda axes over a Cartesian process grid
+(one axis: slabs; several: pencils), src/cpp/slab_nd.cpp:71-254 and
+shafft_internal.cpp:62-127, 229-381.  torch.distributed carries the
+exchanges (NCCL between GPUs; a gloo group exchanges through host memory);
+everything on the device goes through the kernel library:
 
-  forward  local slab [ln0, n1, ..., n_{d-1}] (axis 0 block-partitioned)
-           1. transform axes 1..d-1        (shafft_sm100_plan_create_axes)
-           2. pack the P column blocks of the last axis (shafft_sm100_pack_blocks)
-           3. all-to-all                   (torch.distributed.all_to_all_single)
-              -> [n0, n1, ..., ln_{d-1}]   (last axis block-partitioned;
-                 blocks arrive as row ranges of axis 0, so no unpack)
-           4. transform axis 0
-           with TransformLayout INITIAL the exchange is then undone
-  backward the same steps in reverse (all-to-all of row ranges, then unpack)
+  stage 0        the leading nda axes block-partitioned over the grid
+  subplan s      transforms the contiguous axes not yet transformed
+                 (shafft_sm100_plan_create_axes on the local block)
+  exchange i     inside the grid line of cart dimension nda-1-i: the
+                 distributed axis b of that slot becomes contiguous and the
+                 contiguous axis a = b + nca (nca = ndim - nda) becomes
+                 distributed -- pack the local block along a into per-peer
+                 blocks (shafft_sm100_pack_blocks), all-to-all, unpack along
+                 b (skipped when b is the outermost axis)
+  sequences      subplans alternate with ceil(nda / nca) sequences of up to
+                 nca exchanges; after the last one the layout is
+                 REDISTRIBUTED (TransformLayout INITIAL replays the exchanges
+                 backwards); backward runs the same steps in reverse
 
-which follows FFTNDPlan::executeImpl (src/cpp/shafft_internal.cpp:62-127):
-the same subplan order, the same per-stage layouts (block partition with the
-first n % P parts one element longer, detail/partition.hpp:40-44), the same
-buffer-swap contract (the result is in the buffer get_buffers() reports as
-data) and the (1/sqrt(N))^k normalisation.  Methods return the reference's
-status codes.  More than one distributed axis (pencils) returns
-ERR_NOT_IMPL.  Ranks beyond prod(commDims) are inactive: they own no data
-and take part in the exchanges with empty blocks.  FFT1D (below) is the
-reference's distributed 1-D transform (the P x P four-step path).
+with the reference's block partition (the first n % P parts one element
+longer, detail/partition.hpp:40-44), buffer-swap contract (the result is in
+the buffer get_buffers() reports as data) and (1/sqrt(N))^k normalisation.
+Methods return the reference's status codes.  Ranks beyond prod(commDims)
+are inactive: they own no data and belong to no grid line.  FFT1D (below) is
+the reference's distributed 1-D transform (the P x P four-step path).
 """
 from __future__ import annotations
 
 import ctypes
+import itertools
 import math
 
 from . import (BACKWARD, C2C, ERR_ALLOC, ERR_DIM_MISMATCH, ERR_INVALID_DECOMP, ERR_INVALID_DIM,
@@ -45,68 +49,102 @@ def block_partition(total: int, nparts: int, rank: int):
 
 
 class SlabLayout:
-    """Index bookkeeping of a slab decomposition with one distributed axis:
-    stage 0 splits axis 0, stage 1 (after the forward exchange) splits the
-    last axis.  Pure host arithmetic."""
+    """Index bookkeeping of the decomposition (pure host arithmetic): the
+    distributed / contiguous axes, local block (subsize, offset) of every
+    exchange index 0..nda, the exchanges' axes and grid dimensions, and the
+    exchange sequences with the axes each subplan transforms."""
 
-    def __init__(self, dims, nparts: int, rank: int):
+    def __init__(self, dims, comm_dims, rank: int):
         self.dims = tuple(int(d) for d in dims)
-        self.P = int(nparts)
+        self.comm_dims = [int(c) for c in comm_dims]
+        d = len(self.dims)
+        nda = 0
+        for c in self.comm_dims:
+            if c > 1:
+                nda += 1
+            else:
+                break
+        self.nda, self.nca = nda, d - nda
+        self.grid = self.comm_dims[:nda]
+        self.P = math.prod(self.grid) if nda else 1
         self.rank = int(rank)
         self.active = self.rank < self.P
-        d = len(self.dims)
-        self.mid = math.prod(self.dims[1:-1]) if d > 2 else 1
-        self.sub = []
-        self.off = []
-        for axis in ((0, d - 1) if self.P > 1 else (0,)):
+        # cart coordinates, row-major over the grid (MPI_Cart_create, no reorder)
+        self.coords, r = [], self.rank
+        for g in reversed(self.grid):
+            self.coords.insert(0, r % g if self.active else 0)
+            r //= g
+        das, cas = [list(range(nda))], [list(range(nda, d))]
+        self.axes_a, self.axes_b = [], []
+        for i in range(nda):
+            da, ca = list(das[-1]), list(cas[-1])
+            b = da[nda - i - 1]
+            a = b + self.nca
+            da[nda - i - 1] = a
+            ca[ca.index(a)] = b
+            das.append(da)
+            cas.append(ca)
+            self.axes_a.append(a)
+            self.axes_b.append(b)
+        self.das, self.cas = das, cas
+        self.sub, self.off = [], []
+        for s in range(nda + 1):
             sub, off = list(self.dims), [0] * d
-            if self.P > 1:
-                n, s = block_partition(self.dims[axis], self.P, self.rank) if self.active else (0, 0)
-                sub[axis], off[axis] = n, s
+            for j in range(nda):
+                ax = das[s][j]
+                n, st = block_partition(self.dims[ax], self.grid[j], self.coords[j]) if self.active else (0, 0)
+                sub[ax], off[ax] = n, st
             self.sub.append(sub)
             self.off.append(off)
+        nes = -(-nda // self.nca) if nda else 0
+        self.es = [min(self.nca, nda - i * self.nca) for i in range(nes)]
+        done, self.tf_axes, self.plan_index = set(), [], []
+        for s in range(nes + 1):
+            idx = sum(self.es[:s])
+            ta = [a for a in cas[idx] if a not in done]
+            done.update(ta)
+            self.tf_axes.append(ta)
+            self.plan_index.append(idx)
 
-    @property
-    def nstages(self):
-        return len(self.sub)
-
-    def size(self, stage: int) -> int:
-        return math.prod(self.sub[stage]) if self.active else 0
+    def size(self, idx: int) -> int:
+        return math.prod(self.sub[idx]) if self.active else 0
 
     def alloc_size(self) -> int:
-        return max(self.size(s) for s in range(self.nstages))
+        return max(self.size(s) for s in range(self.nda + 1))
 
-    def axes(self, stage: int):
-        """(contiguous axes, distributed axes) of a stage."""
-        d = len(self.dims)
-        if self.P == 1:
-            return list(range(d)), []
-        return (list(range(1, d)), [0]) if stage == 0 else (list(range(d - 1)), [d - 1])
+    def grid_line(self, j):
+        """World ranks of this rank's grid line along cart dimension j."""
+        out = []
+        for c in range(self.grid[j]):
+            co = list(self.coords)
+            co[j] = c
+            r = 0
+            for g, x in zip(self.grid, co):
+                r = r * g + x
+            out.append(r)
+        return out
 
-    def transform_axes(self, stage: int):
-        """Axes the stage's subplan transforms (contiguous and not yet done)."""
-        d = len(self.dims)
-        if self.P == 1:
-            return list(range(d))
-        return list(range(1, d)) if stage == 0 else [0]
-
-    def forward_counts(self):
-        """(send counts, receive counts) in elements per peer, stage 0 -> 1;
-        the backward exchange swaps the two lists."""
-        send, recv = [], []
-        ln0 = self.sub[0][0]
-        for p in range(self.P):
-            send.append(ln0 * self.mid * block_partition(self.dims[-1], self.P, p)[0]
-                        if self.active else 0)
-            recv.append(block_partition(self.dims[0], self.P, p)[0] * self.mid * self.sub[1][-1]
-                        if self.active else 0)
-        return send, recv
+    def exchange(self, i):
+        """Exchange i (stage i -> i+1): (cart dim, axis a, axis b, Q,
+        pack geometry of stage i along a, unpack geometry of stage i+1 along
+        b, send counts, receive counts); the backward exchange swaps roles."""
+        j = self.nda - i - 1
+        a, b = self.axes_a[i], self.axes_b[i]
+        Q = self.grid[j]
+        sa, sb = self.sub[i], self.sub[i + 1]
+        pack = (math.prod(sa[:a]), self.dims[a], math.prod(sa[a + 1:]))
+        unpack = (math.prod(sb[:b]), self.dims[b], math.prod(sb[b + 1:]))
+        per_a = self.size(i) // self.dims[a] if self.active else 0
+        per_b = self.size(i + 1) // self.dims[b] if self.active else 0
+        send = [per_a * block_partition(self.dims[a], Q, q)[0] for q in range(Q)]
+        recv = [per_b * block_partition(self.dims[b], Q, q)[0] for q in range(Q)]
+        return j, a, b, Q, pack, unpack, send, recv
 
 
 class FFTND:
-    """Distributed shafft::FFTND (one distributed axis) over a
-    torch.distributed process group; buffers are torch CUDA tensors of at
-    least alloc_size() complex elements."""
+    """Distributed shafft::FFTND over a torch.distributed process group;
+    buffers are torch CUDA tensors of at least alloc_size() complex
+    elements."""
 
     def __init__(self):
         self._state = "created"
@@ -140,19 +178,38 @@ class FFTND:
                 break
         if any(c > 1 for c in comm_dims[nda:]):
             return ERR_INVALID_DECOMP
-        if nda > 1:
-            return ERR_NOT_IMPL  # pencil decompositions (several distributed axes)
+        nca = ndim - nda
+        # cross-axis rule: grid dimension j later partitions axis j + nca
+        if any(comm_dims[j] > dims[j + nca] for j in range(nda)):
+            return ERR_INVALID_DECOMP
         world = dist.get_world_size(group) if dist.is_initialized() else 1
         rank = dist.get_rank(group) if dist.is_initialized() else 0
         if ndim == 1 and world > 1:
             return ERR_INVALID_DECOMP
-        P = comm_dims[0]
-        if P > world or (nda == 1 and P > dims[-1]):
+        if math.prod(comm_dims[:nda] or [1]) > world:
             return ERR_INVALID_DECOMP
         self.dims, self.precision, self.group = tuple(dims), precision, group
         self.output_policy = output_policy
         self.world, self.rank = world, rank
-        self.layout = SlabLayout(dims, P, rank)
+        self.layout = SlabLayout(dims, comm_dims, rank)
+        # one process group per grid line (created by every rank, same order)
+        self.lines = {}
+        if self.layout.nda and world > 1:
+            L = self.layout
+            for j in range(L.nda):
+                others = [range(g) for k, g in enumerate(L.grid) if k != j]
+                for rest in itertools.product(*others):
+                    members = []
+                    for c in range(L.grid[j]):
+                        co = list(rest)
+                        co.insert(j, c)
+                        r = 0
+                        for g, x in zip(L.grid, co):
+                            r = r * g + x
+                        members.append(r)
+                    grp = dist.new_group(members) if len(members) < world else group
+                    if L.active and members == L.grid_line(j):
+                        self.lines[j] = grp
         self.ops = device_ops
         self.stage = 0
         self._state = "configured"
@@ -165,10 +222,11 @@ class FFTND:
             return ERR_INVALID_STATE
         if self.ops is None:
             self.ops = CudaOps(self.precision)
+        L = self.layout
         self.subplans = []
-        if self.layout.active:
-            for s in range(self.layout.nstages):
-                self.subplans.append(self.ops.plan(self.layout.sub[s], self.layout.transform_axes(s)))
+        if L.active:
+            for s, idx in enumerate(L.plan_index):
+                self.subplans.append(self.ops.plan(L.sub[idx], L.tf_axes[s]))
         self.data = self.work = None
         self._state = "planned"
         return 0
@@ -199,27 +257,26 @@ class FFTND:
         return 0, self.data, self.work
 
     # layout queries (shafft.hpp:252-265) -------------------------------------
-    def _stage_of(self, which):
+    def _index_of(self, which):
         if which == TENSOR_LAYOUT_CURRENT:
             return self.stage
         if which == TENSOR_LAYOUT_INITIAL:
             return 0
         if which == TENSOR_LAYOUT_REDISTRIBUTED:
-            return self.layout.nstages - 1
+            return self.layout.nda
         return None
 
     def get_layout(self, which=TENSOR_LAYOUT_CURRENT):
-        s = self._stage_of(which)
+        s = self._index_of(which)
         if s is None:
             return ERR_INVALID_LAYOUT, [], []
         return 0, list(self.layout.sub[s]), list(self.layout.off[s])
 
     def get_axes(self, which=TENSOR_LAYOUT_CURRENT):
-        s = self._stage_of(which)
+        s = self._index_of(which)
         if s is None:
             return ERR_INVALID_LAYOUT, [], []
-        ca, da = self.layout.axes(s)
-        return 0, ca, da
+        return 0, list(self.layout.cas[s]), list(self.layout.das[s])
 
     # compute ---------------------------------------------------------------
     def _fft(self, s, direction):
@@ -227,48 +284,58 @@ class FFTND:
         self.data, self.work = self.work, self.data
 
     def _exchange(self, forward):
-        """stage 0 -> 1 (forward) or 1 -> 0; the result is left in data."""
-        send, recv = self.layout.forward_counts()
-        if not forward:
-            send, recv = recv, send
-        # ranks beyond the P active ones exchange empty blocks
-        pad = [0] * (self.world - len(send))
-        send, recv = send + pad, recv + pad
+        """One exchange from the current stage (forward: i = stage; backward:
+        i = stage - 1); the result is left in data."""
         L = self.layout
-        n_last = self.dims[-1]
-        if forward:
-            if L.active:
-                self.ops.pack(self.data, self.work, L.sub[0][0] * L.mid, n_last, L.P)
-            self.ops.alltoall(self.data, self.work, recv, send, self.group, self.world)
+        i = self.stage if forward else self.stage - 1
+        j, a, b, Q, pack, unpack, send, recv = L.exchange(i)
+        if not forward:
+            pack, unpack, send, recv = unpack, pack, recv, send
+        grp = self.lines.get(j, self.group)
+        if pack[0] == 1:  # blocks along the outermost axis are row ranges
+            src = self.data
         else:
-            self.ops.alltoall(self.work, self.data, recv, send, self.group, self.world)
-            if L.active:
-                self.ops.unpack(self.work, self.data, L.sub[0][0] * L.mid, n_last, L.P)
-        self.stage = 1 if forward else 0
+            self.ops.pack(self.data, self.work, *pack, Q)
+            src = self.work
+        dst = self.work if src is self.data else self.data
+        self.ops.alltoall(dst, src, recv, send, grp, Q)
+        if unpack[0] == 1:
+            if dst is not self.data:
+                self.data, self.work = self.work, self.data
+        else:
+            out = self.work if dst is self.data else self.data
+            self.ops.unpack(dst, out, *unpack, Q)
+            if out is not self.data:
+                self.data, self.work = self.work, self.data
+        self.stage = i + 1 if forward else i
 
     def execute(self, direction) -> int:
         if self._state != "planned":
             return ERR_PLAN_NOT_INIT
-        if self.layout.active and (self.data is None or self.work is None):
+        L = self.layout
+        if not L.active:
+            self.norm_exponent += 1
+            return 0
+        if self.data is None or self.work is None:
             return ERR_NO_BUFFER
-        last = self.layout.nstages - 1
+        nes = len(L.es)
         if direction == FORWARD:
-            for s in range(self.layout.nstages):
-                if self.layout.active:
-                    self._fft(s, FORWARD)
-                if s < last:
-                    self._exchange(True)
+            for s in range(nes + 1):
+                self._fft(s, FORWARD)
+                if s < nes:
+                    for _ in range(L.es[s]):
+                        self._exchange(True)
             if self.output_policy == LAYOUT_INITIAL:
                 while self.stage > 0:
                     self._exchange(False)
         elif direction == BACKWARD:
-            while self.stage < last:  # re-apply the redistribution first
+            while self.stage < L.nda:  # re-apply the redistribution first
                 self._exchange(True)
-            for s in range(last, -1, -1):
-                if self.layout.active:
-                    self._fft(s, BACKWARD)
+            for s in range(nes, -1, -1):
+                self._fft(s, BACKWARD)
                 if s > 0:
-                    self._exchange(False)
+                    for _ in range(L.es[s - 1]):
+                        self._exchange(False)
         else:
             return ERR_INVALID_STATE
         self.norm_exponent += 1
@@ -387,7 +454,7 @@ class FFT1D:
             self.ops.alltoall(x, s, eq, eq, self.group, P)              # 4
             self.ops.execute(self.plans[1], x, s, direction)            # 5  X[r + P k2]
             self.ops.alltoall(x, s, eq, eq, self.group, P)              # 6  [s][j]
-            self.ops.unpack(x, w, C, P, P)                              # 7  [j][s]
+            self.ops.unpack(x, w, C, P, 1, P)                           # 7  [j][s]
         self.data, self.work = w, x
         self.norm_exponent += 1
         return 0
@@ -428,7 +495,7 @@ class CudaOps:
             ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         for f in (self.lib.shafft_sm100_pack_blocks, self.lib.shafft_sm100_unpack_blocks):
             f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
-                          ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+                          ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         self.precision = precision
         self.torch = torch
 
@@ -453,13 +520,14 @@ class CudaOps:
                                                       ctypes.c_double(1.0), self._stream()),
                         "execute")
 
-    def pack(self, src, dst, outer, n, P):
-        self._sm._check(self.lib.shafft_sm100_pack_blocks(src.data_ptr(), dst.data_ptr(), outer, n, P,
-                                                          self.precision, self._stream()), "pack")
+    def pack(self, src, dst, outer, n, inner, P):
+        self._sm._check(self.lib.shafft_sm100_pack_blocks(src.data_ptr(), dst.data_ptr(), outer, n, inner,
+                                                          P, self.precision, self._stream()), "pack")
 
-    def unpack(self, src, dst, outer, n, P):
-        self._sm._check(self.lib.shafft_sm100_unpack_blocks(src.data_ptr(), dst.data_ptr(), outer, n, P,
-                                                            self.precision, self._stream()), "unpack")
+    def unpack(self, src, dst, outer, n, inner, P):
+        self._sm._check(self.lib.shafft_sm100_unpack_blocks(src.data_ptr(), dst.data_ptr(), outer, n,
+                                                            inner, P, self.precision, self._stream()),
+                        "unpack")
 
     def twiddle(self, data, rows, cols, col0, n, sign):
         self._sm._check(self.lib.shafft_sm100_twiddle_rows(data.data_ptr(), rows, cols, col0, n, sign,

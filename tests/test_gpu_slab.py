@@ -45,19 +45,20 @@ def test_axis_subset_plans_vs_oracle(dims, axes, prec):
     ops.destroy(h)
 
 
-@pytest.mark.parametrize("outer,n,P", [(6, 48, 2), (5, 7, 3), (1, 10, 4), (33, 64, 8)])
-def test_pack_unpack_blocks(outer, n, P):
+@pytest.mark.parametrize("outer,n,inner,P", [(6, 48, 1, 2), (5, 7, 1, 3), (1, 10, 1, 4), (33, 64, 1, 8),
+                                             (4, 10, 6, 3), (3, 7, 5, 2)])
+def test_pack_unpack_blocks(outer, n, inner, P):
     from shafft_b200.slab import CudaOps, block_partition
     import torch
     ops = CudaOps(S.C2C)
-    x = o.uniform_input((outer, n), seed=1, dtype=np.complex64)
+    x = o.uniform_input((outer, n, inner), seed=1, dtype=np.complex64)
     a = torch.from_numpy(x.ravel()).cuda()
     b = torch.empty_like(a)
     c = torch.empty_like(a)
-    ops.pack(a, b, outer, n, P)
-    ops.unpack(b, c, outer, n, P)
+    ops.pack(a, b, outer, n, inner, P)
+    ops.unpack(b, c, outer, n, inner, P)
     torch.cuda.synchronize()
-    want = np.concatenate([x[:, s:s + l].ravel() for l, s in (block_partition(n, P, p) for p in range(P))])
+    want = np.concatenate([x[:, s:s + l, :].ravel() for l, s in (block_partition(n, P, p) for p in range(P))])
     assert np.array_equal(b.cpu().numpy(), want)
     assert np.array_equal(c.cpu().numpy(), x.ravel())
 
@@ -73,11 +74,12 @@ cfg = json.loads(sys.argv[3])
 torch.cuda.set_device(0)
 dist.init_process_group("gloo")
 dims, prec, P = tuple(cfg["dims"]), cfg["prec"], cfg["P"]
+cdims = cfg.get("comm_dims") or [P] + [1] * (len(dims) - 1)
 dt = np.complex128 if prec == S.Z2Z else np.complex64
 g = o.uniform_input(dims, seed=42, dtype=dt)
 ref = o.fftn(g.astype(np.complex128), precise=(prec == S.Z2Z))
 plan = slab.FFTND()
-assert plan.init([P] + [1] * (len(dims) - 1), dims, prec, None, cfg["policy"]) == 0
+assert plan.init(cdims, dims, prec, None, cfg["policy"]) == 0
 assert plan.plan() == 0
 n = plan.alloc_size()
 tdt = torch.complex128 if prec == S.Z2Z else torch.complex64
@@ -116,11 +118,24 @@ def _free_port():
                                               ((97, 36, 10), S.C2C, S.LAYOUT_INITIAL),
                                               ((128, 96), S.C2C, S.LAYOUT_REDISTRIBUTED)])
 def test_distributed_fftnd_two_ranks(tmp_path, dims, prec, policy):
-    world = 2
+    _run_nd(tmp_path, 2, {"dims": list(dims), "prec": prec, "P": 2, "policy": policy})
+
+
+@pytest.mark.parametrize("dims,prec,policy", [((64, 48, 40), S.C2C, S.LAYOUT_REDISTRIBUTED),
+                                              ((30, 28, 26), S.Z2Z, S.LAYOUT_INITIAL)])
+def test_pencil_fftnd_four_ranks(tmp_path, dims, prec, policy):
+    """commDims [2, 2, 1]: two exchange sequences inside 2-rank grid lines."""
+    res = _run_nd(tmp_path, 4, {"dims": list(dims), "prec": prec, "P": 2, "comm_dims": [2, 2, 1],
+                                "policy": policy})
+    if policy == S.LAYOUT_REDISTRIBUTED:  # full axis 0, axes 1 and 2 in blocks
+        assert all(x["fwd_layout"][0][0] == dims[0] for x in res)
+
+
+def _run_nd(tmp_path, world, cfg):
+    dims, prec, policy = tuple(cfg["dims"]), cfg["prec"], cfg["policy"]
     script = tmp_path / "worker.py"
     script.write_text(WORKER)
     port = _free_port()
-    cfg = {"dims": list(dims), "prec": prec, "P": world, "policy": policy}
     procs = []
     for r in range(world):
         env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
@@ -136,12 +151,13 @@ def test_distributed_fftnd_two_ranks(tmp_path, dims, prec, policy):
     back = math.sqrt(sum(x["bt2"] for x in res) / sum(x["g2"] for x in res))
     assert err <= tol(n, prec), err
     assert back <= 2 * tol(n, prec), back
-    if policy == S.LAYOUT_REDISTRIBUTED:
-        # forward output: full axis 0, the last axis in blocks
+    if policy == S.LAYOUT_REDISTRIBUTED and "comm_dims" not in cfg:
+        # slab forward output: full axis 0, the last axis in blocks
         assert all(x["fwd_layout"][0][0] == dims[0] for x in res)
         assert sum(x["fwd_layout"][0][-1] for x in res) == dims[-1]
-    else:
+    elif "comm_dims" not in cfg:
         assert sum(x["fwd_layout"][0][0] for x in res) == dims[0]
+    return res
 
 
 WORKER_1D = r'''

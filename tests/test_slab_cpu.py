@@ -39,16 +39,17 @@ class NumpyOps:
         else:
             y = np.fft.ifftn(x, axes=axes) * math.prod(dims[a] for a in axes)
         dst[:n] = torch.from_numpy(y.ravel())
-    def pack(self, src, dst, outer, n, P):
-        a = src[:outer * n].numpy().reshape(outer, n)
-        parts = [a[:, s:s + l].ravel() for l, s in (slab.block_partition(n, P, p) for p in range(P))]
-        dst[:outer * n] = torch.from_numpy(np.concatenate(parts))
-    def unpack(self, src, dst, outer, n, P):
-        out = np.empty((outer, n), dtype=np.complex128); pos = 0
+    def pack(self, src, dst, outer, n, inner, P):
+        a = src[:outer * n * inner].numpy().reshape(outer, n, inner)
+        parts = [a[:, s:s + l, :].ravel() for l, s in (slab.block_partition(n, P, p) for p in range(P))]
+        dst[:outer * n * inner] = torch.from_numpy(np.concatenate(parts))
+    def unpack(self, src, dst, outer, n, inner, P):
+        out = np.empty((outer, n, inner), dtype=np.complex128); pos = 0
         for p in range(P):
             l, s = slab.block_partition(n, P, p)
-            out[:, s:s + l] = src[pos:pos + outer * l].numpy().reshape(outer, l); pos += outer * l
-        dst[:outer * n] = torch.from_numpy(out.ravel())
+            out[:, s:s + l, :] = src[pos:pos + outer * l * inner].numpy().reshape(outer, l, inner)
+            pos += outer * l * inner
+        dst[:outer * n * inner] = torch.from_numpy(out.ravel())
     def scale(self, data, count, f): data[:count] *= f
     def twiddle(self, data, rows, cols, col0, n, sign):
         k = np.arange(rows)[:, None]; c = np.arange(cols)[None, :]
@@ -86,11 +87,12 @@ if cfg.get("fft1d"):
     json.dump(out, open(sys.argv[2], "w"))
     sys.exit(0)
 dims = tuple(cfg["dims"]); P = cfg["P"]
+cdims = cfg.get("comm_dims") or [P] + [1] * (len(dims) - 1)
 rng = np.random.Generator(np.random.MT19937(5))
 g = rng.uniform(-1, 1, dims) + 1j * rng.uniform(-1, 1, dims)
 f = S.__dict__
 plan = slab.FFTND()
-rc = plan.init([P] + [1] * (len(dims) - 1), dims, S.Z2Z, None, cfg["policy"], device_ops=NumpyOps())
+rc = plan.init(cdims, dims, S.Z2Z, None, cfg["policy"], device_ops=NumpyOps())
 assert rc == 0, rc
 assert plan.plan() == 0
 n = plan.alloc_size()
@@ -149,17 +151,39 @@ def test_slab_fftnd_on_gloo_ranks(tmp_path, world, dims, policy):
         assert o["rt_err"] < 1e-12, o
 
 
-def test_inactive_rank_takes_part_with_empty_blocks(tmp_path):
-    """commDims product below the group size: the extra rank owns nothing."""
+def test_inactive_rank_owns_nothing(tmp_path):
+    """commDims product below the group size: the extra rank owns nothing and
+    belongs to no grid line."""
     res = _run(tmp_path, 3, {"dims": [4, 3, 5], "P": 2, "policy": 0})
     assert all(o["fwd_err"] < 1e-12 and o["rt_err"] < 1e-12 for o in res)
 
 
+@pytest.mark.parametrize("world,comm_dims,dims,policy", [
+    (4, [2, 2, 1], (8, 6, 10), 0),        # pencils: two exchange sequences
+    (4, [2, 2, 1], (7, 5, 6), 1),         # uneven blocks, INITIAL output
+    (6, [2, 3, 1], (8, 6, 10), 0),        # unequal grid dimensions
+    (4, [2, 2, 1, 1], (8, 6, 10, 4), 0),  # nca = 2: one sequence of two exchanges
+    (5, [2, 2, 1], (6, 4, 5), 1)])        # one inactive rank
+def test_pencil_fftnd_on_gloo_ranks(tmp_path, world, comm_dims, dims, policy):
+    res = _run(tmp_path, world, {"dims": list(dims), "P": comm_dims[0], "comm_dims": comm_dims,
+                                 "policy": policy})
+    for o in res:
+        assert o["fwd_err"] < 1e-12, o
+        assert o["rt_err"] < 1e-12, o
+
+
 def test_layout_bookkeeping_matches_reference_partition():
-    L = slab.SlabLayout((6, 5, 7), 3, 1)
+    L = slab.SlabLayout((6, 5, 7), [3, 1, 1], 1)
     assert L.sub == [[2, 5, 7], [6, 5, 2]] and L.off == [[2, 0, 0], [0, 0, 3]]
     assert L.alloc_size() == 70
-    assert L.forward_counts() == ([30, 20, 20], [20, 20, 20])
+    j, a, b, Q, pack, unpack, send, recv = L.exchange(0)
+    assert (j, a, b, Q) == (0, 2, 0, 3) and pack == (10, 7, 1) and unpack[0] == 1
+    assert (send, recv) == ([30, 20, 20], [20, 20, 20])
+    # pencils: rank 4 of a 2 x 3 grid on 8 x 6 x 10
+    L = slab.SlabLayout((8, 6, 10), [2, 3, 1], 4)
+    assert L.coords == [1, 1] and L.es == [1, 1] and L.tf_axes == [[2], [1], [0]]
+    assert L.sub == [[4, 2, 10], [4, 6, 3], [8, 3, 3]]
+    assert L.das == [[0, 1], [0, 2], [1, 2]] and L.grid_line(0) == [1, 4] and L.grid_line(1) == [3, 4, 5]
     assert [slab.block_partition(10, 4, r) for r in range(4)] == [(3, 0), (3, 3), (2, 6), (2, 8)]
 
 
@@ -172,7 +196,9 @@ def test_init_validation():
     p = slab.FFTND()
     assert p.init([9, 1], [8, 8]) == S.ERR_INVALID_DECOMP       # more parts than rows
     p = slab.FFTND()
-    assert p.init([2, 2, 1], [8, 8, 8]) == S.ERR_NOT_IMPL       # pencils
+    assert p.init([2, 2, 1], [8, 8, 8]) == S.ERR_INVALID_DECOMP  # 4 grid ranks, 1 process
+    p = slab.FFTND()
+    assert p.init([2, 9, 1], [8, 9, 8]) == S.ERR_INVALID_DECOMP  # grid dim 1 > axis 2 later
     p = slab.FFTND()
     assert p.init([2, 1], [8, 8]) == S.ERR_INVALID_DECOMP       # 2 parts, 1 process
     p = slab.FFTND()
