@@ -48,6 +48,167 @@ def block_partition(total: int, nparts: int, rank: int):
     return (q + 1, rank * (q + 1)) if rank < r else (q, r * (q + 1) + (rank - r) * q)
 
 
+# ---- decomposition search (the reference's configurationND) ---------------
+# src/cpp/configuration.cpp:94-600, restated: a user grid is validated
+# (configurationCart); a requested number of distributed axes is tried
+# exactly; otherwise d = ndim-1 .. 1 (MAXIMIZE_NDA) or 1 .. ndim-1
+# (MINIMIZE_NDA) is tried: a balanced grid of the world size (as
+# MPI_Dims_create), capped per axis by min(size[i], size[i + ndim - d]),
+# packed greedily into the leading axes (factors fill an axis up to its cap
+# before spilling to the next), accepted when every active rank's block
+# passes the 32-bit element limit and the memory limit (two buffers).  Every
+# rank's block is computed locally, so no reduction across ranks is needed.
+
+MAXIMIZE_NDA, MINIMIZE_NDA = 0, 1
+
+
+def _dims_create(n, d):
+    """Balanced factorisation of n into d factors, non-increasing (the
+    result MPI_Dims_create gives for an all-zero dims array)."""
+    primes, m, f = [], n, 2
+    while f * f <= m:
+        while m % f == 0:
+            primes.append(f)
+            m //= f
+        f += 1
+    if m > 1:
+        primes.append(m)
+    dims = [1] * d
+    for p in sorted(primes, reverse=True):
+        i = dims.index(min(dims))
+        dims[i] *= p
+    return sorted(dims, reverse=True)
+
+
+def _min_caps(ndim, d, sizes):
+    return [min(sizes[i], sizes[i + ndim - d]) for i in range(d)]
+
+
+def _largest_divisor_leq(n, limit):
+    if n <= 1 or limit < 2:
+        return 1
+    return max(x for x in range(1, min(n, limit) + 1) if n % x == 0)
+
+
+def _pack_prefix_with_spill(ndim, grid, sizes, caps):
+    factors = [g for g in grid if g > 1]
+    grid[:] = [1] * ndim
+    max_axes = max(0, ndim - 1)
+    cap_left = [max(1, min(sizes[i], caps[i]) if caps and i < len(caps) else sizes[i])
+                for i in range(max_axes)]
+    axis = 0
+    for f in factors:
+        rem = f
+        while rem > 1 and axis < max_axes:
+            room = cap_left[axis] // grid[axis]
+            if room < 2:
+                axis += 1
+                continue
+            used = _largest_divisor_leq(rem, room)
+            if used <= 1:
+                axis += 1
+                continue
+            grid[axis] *= used
+            rem //= used
+            if grid[axis] == cap_left[axis]:
+                axis += 1
+    dp = 0
+    while dp < max_axes and grid[dp] > 1:
+        dp += 1
+    for i in range(dp, ndim):
+        grid[i] = 1
+    return dp
+
+
+def _blocks_ok(dims, d, grid, precision, mem_limit):
+    """Every active rank's block within the 32-bit element limit and the
+    memory limit (two buffers of the local block)."""
+    ndim = len(dims)
+    esize = 8 if precision == C2C else 16
+    for rank in range(math.prod(grid[:d]) if d else 1):
+        coords, r = [], rank
+        for g in reversed(grid[:d]):
+            coords.insert(0, r % g)
+            r //= g
+        sub = list(dims)
+        for i in range(d):
+            sub[i] = block_partition(dims[i], grid[i], coords[i])[0]
+        n = math.prod(sub)
+        if min(sub) <= 0 or n > 2 ** 31 - 1:
+            return False
+        if mem_limit and 2 * esize * n > mem_limit:
+            return False
+    return True
+
+
+def configuration_nd(dims, world, rank=0, precision=C2C, comm_dims=None, nda=0,
+                     strategy=MAXIMIZE_NDA, mem_limit=0):
+    """(status, commDims, nda, subsize, offset, active ranks) for `world`
+    ranks, as the reference's shafft::configurationND
+    (src/cpp/configuration.cpp:530-600)."""
+    ndim = len(dims)
+    sizes = [int(x) for x in dims]
+    grid = [int(c) for c in (comm_dims or [0] * ndim)]
+    if len(grid) != ndim:
+        return ERR_DIM_MISMATCH, None, 0, None, None, 0
+
+    def result(g, d):
+        L = SlabLayout(sizes, g, rank)
+        act = math.prod(g[:d]) if d else 1
+        return 0, list(g), d, list(L.sub[0]), list(L.off[0]), act
+
+    if any(grid) and all(c > 0 for c in grid):  # a user grid (configurationCart)
+        d = 0
+        while d < ndim and grid[d] > 1:
+            d += 1
+        ok = d < ndim and all(c == 1 for c in grid[d:])
+        if d == 0:
+            ok = world == 1
+        if ok and d:
+            caps = _min_caps(ndim, d, sizes)
+            ok = all(1 <= grid[i] <= min(sizes[i], caps[i]) for i in range(d)) and math.prod(grid[:d]) <= world
+        if ok and _blocks_ok(sizes, d, grid, precision, mem_limit):
+            return result(grid, d)
+
+    def try_d(d, strict):
+        if d < 1 or d > ndim - 1:
+            return None
+        g = [1] * ndim
+        caps = _min_caps(ndim, d, sizes)
+        if d == 1:
+            g[0] = min(world, sizes[0])
+        else:
+            md = _dims_create(world, d)
+            for i in range(d):
+                g[i] = max(1, min(md[i], caps[i]))
+        if strict and sum(1 for i in range(d) if g[i] > 1) != d:
+            return None
+        de = d
+        if not strict:
+            de = _pack_prefix_with_spill(ndim, g, sizes, caps)
+            if de == 0 and world > 1:
+                return None
+            if de != d:
+                caps2 = _min_caps(ndim, de, sizes)
+                if any(g[i] > caps2[i] for i in range(de)):
+                    return None
+        if not _blocks_ok(sizes, de, g, precision, mem_limit):
+            return None
+        return g, de
+
+    if nda > 0:
+        r = try_d(nda, True)
+        return result(*r) if r else (ERR_INVALID_DECOMP, None, 0, None, None, 0)
+    order = range(ndim - 1, 0, -1) if strategy == MAXIMIZE_NDA else range(1, ndim)
+    for d in order:
+        r = try_d(d, False)
+        if r:
+            return result(*r)
+    if world == 1:
+        return result([1] * ndim, 0)
+    return ERR_INVALID_DECOMP, None, 0, None, None, 0
+
+
 class SlabLayout:
     """Index bookkeeping of the decomposition (pure host arithmetic): the
     distributed / contiguous axes, local block (subsize, offset) of every

@@ -219,3 +219,28 @@ def test_slab_fft1d_needs_p_squared(tmp_path):
     import shafft_b200 as S
     res = _run(tmp_path, 2, {"fft1d": True, "n": 6})   # 6 % 4 != 0
     assert all(o["init"] == S.ERR_NOT_IMPL for o in res)
+
+
+def test_configuration_nd_decomposition_search():
+    """The restated configurationND: one rank resolves to all ones with
+    nda 0 (the reference's single-rank result); slabs are preferred until
+    per-axis caps force a second distributed axis; a requested nda is tried
+    exactly; a valid user grid is kept, an invalid one falls back to the
+    search; memory limits reject blocks that are too large."""
+    cfg = slab.configuration_nd
+    assert cfg((64, 64, 32), 1)[:3] == (0, [1, 1, 1], 0)
+    assert cfg((64, 64, 32), 4)[:3] == (0, [4, 1, 1], 1)
+    assert cfg((64, 64, 32), 4, strategy=slab.MINIMIZE_NDA)[:3] == (0, [4, 1, 1], 1)
+    assert cfg((4, 64, 64), 8)[:3] == (0, [4, 2, 1], 2)
+    assert cfg((8, 8, 8), 64)[:3] == (0, [8, 8, 1], 2)
+    assert cfg((64, 64, 32), 4, nda=2)[:3] == (0, [2, 2, 1], 2)
+    assert cfg((64, 64, 32), 4, comm_dims=[2, 2, 1])[:3] == (0, [2, 2, 1], 2)
+    assert cfg((64, 64, 32), 3, comm_dims=[2, 2, 1])[:3] == (0, [3, 1, 1], 1)  # 4 > 3 ranks
+    st, g, d, sub, off, act = cfg((10, 6, 4), 4, rank=3)
+    assert (g, d, sub, off, act) == ([4, 1, 1], 1, [2, 6, 4], [8, 0, 0], 4)
+    # 64^3 complex64 in two buffers over 2 ranks needs 2 MiB each: a 1 MiB
+    # limit forces more ranks' worth of splitting than 2 can give
+    assert cfg((64, 64, 64), 2, mem_limit=1 << 20)[0] != 0
+    assert cfg((64, 64, 64), 2, mem_limit=4 << 20)[:3] == (0, [2, 1, 1], 1)
+    assert [slab._dims_create(n, d) for n, d in ((4, 2), (12, 2), (8, 3), (6, 2))] == \
+        [[2, 2], [4, 3], [2, 2, 2], [3, 2]]
