@@ -18,6 +18,10 @@ int report_error(int code, const char* msg);
 // int set to 1 when a wait for the tensor core gives up.
 bool tc_supported(const PassGeom& g);
 size_t tc_smem_bytes(int L);
+// bytes of the split DFT matrix of length L, and its generation (FP64 phases,
+// FP16 hi/lo split, in the layout k_fft_tc copies into shared memory)
+size_t tc_table_bytes(int L);
+int tc_gen_table(void* dst, int L, cudaStream_t s);
 template <typename C>
 struct PassTables;
 int tc_pass(const PassGeom& g, const float2* in, float2* out, const PassTables<float2>& tb, int* err,

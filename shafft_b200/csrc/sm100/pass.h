@@ -117,6 +117,7 @@ struct PassTables {
   const uint16_t* k2p;     // frequency index -> position
   const C* tw_hi;          // w_N^{(m >> shift) << shift}
   const C* tw_lo;          // w_N^{m & mask}
+  const void* tcB;         // tensor-core passes: split DFT matrix in shared-memory layout
 };
 
 }  // namespace shafft_sm100

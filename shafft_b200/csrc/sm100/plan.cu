@@ -110,6 +110,7 @@ struct Step {
 struct LTable {
   int L;
   size_t off_tw, off_p2k, off_k2p;
+  size_t off_tcB = 0, tc_bytes = 0;  // split DFT matrix of tensor-core passes
 };
 struct NTable {
   int64_t N;
@@ -241,6 +242,11 @@ struct Planner {
     st.tc = 1;
     st.fast = 0;
     st.smem = tc_smem_bytes(st.g.L);
+    LTable& lt = ltabs[st.tabL];
+    if (!lt.tc_bytes) {
+      lt.tc_bytes = tc_table_bytes(st.g.L);
+      lt.off_tcB = alloc(lt.tc_bytes);
+    }
   }
 
   size_t alloc(size_t bytes) {
@@ -916,6 +922,7 @@ struct Launcher {
     tb.twL = reinterpret_cast<const C*>(p->d_tables + lt.off_tw);
     tb.p2k = reinterpret_cast<const uint16_t*>(p->d_tables + lt.off_p2k);
     tb.k2p = reinterpret_cast<const uint16_t*>(p->d_tables + lt.off_k2p);
+    if (lt.tc_bytes) tb.tcB = p->d_tables + lt.off_tcB;
     if (st.tabN >= 0) {
       const NTable& nt = p->ntabs[st.tabN];
       tb.tw_hi = reinterpret_cast<const C*>(p->d_tables + nt.off_hi);
@@ -1025,6 +1032,10 @@ struct Launcher {
   // Build every table of the plan on the device.
   static int build_tables(shafft_sm100_plan_s* p) {
     for (const LTable& lt : p->ltabs) {
+      if (lt.tc_bytes) {
+        const int rc = tc_gen_table(p->d_tables + lt.off_tcB, lt.L, p->stream);
+        if (rc) return rc;
+      }
       int rc = check(K::gen_twiddle(reinterpret_cast<C*>(p->d_tables + lt.off_tw), lt.L, 1, lt.L,
                                     p->stream),
                      "twiddle generation");

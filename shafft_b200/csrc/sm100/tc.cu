@@ -250,25 +250,11 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_addr));
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  // DFT matrix, split: element (k, n) = w_L^{nk}, zero outside L x L
-  for (int it = tid; it < G * Lp; it += kTcThreads) {
-    const int k = it % Lp, c = it / Lp;
-    uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-    for (int j = 0; j < 8; j += 2) {
-      float2 w0 = {0.f, 0.f}, w1 = {0.f, 0.f};
-      const int n0 = 8 * c + j;
-      if (k < L && n0 < L) w0 = __ldg(tb.twL + (n0 * k) % L);  // n, k < 64: 32-bit
-      if (k < L && n0 + 1 < L) w1 = __ldg(tb.twL + ((n0 + 1) * k) % L);
-      split2(w0.x, w1.x, rh[j / 2], rl[j / 2]);
-      split2(w0.y, w1.y, ih[j / 2], il[j / 2]);
-    }
-    const uint32_t o = cm_off(k, c, Lp);
-    unsigned char* B = smem + ly.off_b;
-    *reinterpret_cast<uint4*>(B + 0 * ly.b_bytes + o) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-    *reinterpret_cast<uint4*>(B + 1 * ly.b_bytes + o) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-    *reinterpret_cast<uint4*>(B + 2 * ly.b_bytes + o) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-    *reinterpret_cast<uint4*>(B + 3 * ly.b_bytes + o) = make_uint4(il[0], il[1], il[2], il[3]);
+  // DFT matrix, split, built once per plan (k_gen_tc_dft): 16-byte copies
+  {
+    const uint4* src = static_cast<const uint4*>(tb.tcB);
+    uint4* dst = reinterpret_cast<uint4*>(smem + ly.off_b);
+    for (int i = tid; i < (int)(4 * ly.b_bytes / 16); i += kTcThreads) dst[i] = __ldg(src + i);
   }
 
   const int64_t rows_total = g.ext[0] * g.ext[1] * g.ext[2] * g.ext[3];
@@ -462,6 +448,40 @@ __global__ void __launch_bounds__(kTcThreads, 2)
   }
 }
 
+// The split DFT matrix of length L in the shared-memory layout of k_fft_tc
+// (four Lp x Lp FP16 operands Cr_hi, Cr_lo, Ci_hi, Ci_lo, K-major core
+// matrices): element (k, n) = w_L^{nk} with the phase nk mod L reduced in
+// integers and sincospi in FP64, zero outside L x L.
+__global__ void k_gen_tc_dft(unsigned char* dst, int L) {
+  const TcLayout ly = tc_layout(L);
+  const int Lp = ly.Lp, G = Lp / 8;
+  for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < G * Lp; it += gridDim.x * blockDim.x) {
+    const int k = it % Lp, c = it / Lp;
+    uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+    for (int j = 0; j < 8; j += 2) {
+      float w[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int n = 8 * c + j + h;
+        if (k < L && n < L) {
+          double s, co;
+          sincospi(-2.0 * (double)((n * k) % L) / (double)L, &s, &co);
+          w[h][0] = (float)co;
+          w[h][1] = (float)s;
+        }
+      }
+      split2(w[0][0], w[1][0], rh[j / 2], rl[j / 2]);
+      split2(w[0][1], w[1][1], ih[j / 2], il[j / 2]);
+    }
+    const uint32_t o = cm_off(k, c, Lp);
+    *reinterpret_cast<uint4*>(dst + 0 * ly.b_bytes + o) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+    *reinterpret_cast<uint4*>(dst + 1 * ly.b_bytes + o) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+    *reinterpret_cast<uint4*>(dst + 2 * ly.b_bytes + o) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+    *reinterpret_cast<uint4*>(dst + 3 * ly.b_bytes + o) = make_uint4(il[0], il[1], il[2], il[3]);
+  }
+}
+
 uint32_t tc_max_smem() {
   uint32_t m = 0;
   for (int L = 16; L <= kTcMaxLen; L += 16) m = tc_layout(L).total > m ? tc_layout(L).total : m;
@@ -473,6 +493,15 @@ uint32_t tc_max_smem() {
 bool tc_supported(const PassGeom& g) { return g.L >= 2 && g.L <= kTcMaxLen; }
 
 size_t tc_smem_bytes(int L) { return tc_layout(L).total; }
+
+size_t tc_table_bytes(int L) { return 4 * (size_t)tc_layout(L).b_bytes; }
+
+int tc_gen_table(void* dst, int L, cudaStream_t s) {
+  if (L < 2 || L > kTcMaxLen) return report_error(4, "tensor-core table: length outside 2..64");
+  k_gen_tc_dft<<<8, 256, 0, s>>>(static_cast<unsigned char*>(dst), L);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : report_error(3, cudaGetErrorString(e));
+}
 
 int tc_pass(const PassGeom& g, const float2* in, float2* out, const PassTables<float2>& tb, int* err,
             cudaStream_t s) {
