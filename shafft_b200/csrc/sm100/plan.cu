@@ -878,6 +878,9 @@ static void digit_tables(int L, std::vector<uint16_t>& p2k, std::vector<uint16_t
 
 using namespace shafft_sm100;
 
+struct shafft_sm100_plan_s;
+using Plan = shafft_sm100_plan_s;
+
 struct shafft_sm100_plan_s {
   int precision = 0;
   int ndim = 0;
@@ -896,6 +899,22 @@ struct shafft_sm100_plan_s {
   int device = 0;
   int flags = 0;
   size_t off_tcerr = 0;  // tensor-core passes: device error word (0 = ok)
+  // Replayed launch sequences: executes with the same (src, dst, direction,
+  // scale) run as one CUDA graph from the third call on (the first runs
+  // eagerly, the second is captured on a private stream).
+  struct GraphEntry {
+    void* src;
+    void* dst;
+    int dir;
+    double scale;
+    int calls;
+    cudaGraphExec_t exec;
+    uint64_t last;
+  };
+  std::vector<GraphEntry> graphs;
+  cudaStream_t capture_stream = nullptr;
+  bool graphs_off = false;
+  uint64_t graph_clock = 0;
 };
 
 namespace {
@@ -1354,6 +1373,15 @@ Knobs measured_knobs(int ndim, const int64_t* dims, int precision, int flags, ui
   return best;
 }
 
+// SHAFFT_SM100_GRAPHS=0 turns graph replay of executes off
+bool graphs_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("SHAFFT_SM100_GRAPHS");
+    return !(e && atoi(e) == 0);
+  }();
+  return on;
+}
+
 int validate_flags(int flags, int precision) {
   const int tc_flags = SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES;
   if (flags & ~(tc_flags | SHAFFT_SM100_PLAN_MEASURE))
@@ -1452,6 +1480,9 @@ int shafft_sm100_plan_destroy(shafft_sm100_plan plan) {
   int dev = -1;
   cudaGetDevice(&dev);
   if (dev != plan->device) cudaSetDevice(plan->device);
+  for (auto& g : plan->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
   if (plan->d_tables) cudaFree(plan->d_tables);
   if (plan->d_s0) cudaFree(plan->d_s0);
   if (plan->d_s1) cudaFree(plan->d_s1);
@@ -1474,9 +1505,68 @@ int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direc
   if (direction != 0 && direction != 1) return set_err(SHAFFT_SM100_EINVAL, "bad direction");
   cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : plan->stream;
   void* bufs[4] = {src, dst, plan->d_s0, plan->d_s1};
-  return plan->precision
-             ? Launcher<double>::run_steps(plan, plan->steps, bufs, direction == 1, scale, s)
-             : Launcher<float>::run_steps(plan, plan->steps, bufs, direction == 1, scale, s);
+  auto eager = [&](cudaStream_t st) {
+    return plan->precision
+               ? Launcher<double>::run_steps(plan, plan->steps, bufs, direction == 1, scale, st)
+               : Launcher<float>::run_steps(plan, plan->steps, bufs, direction == 1, scale, st);
+  };
+  if (!graphs_enabled() || plan->graphs_off || plan->steps.size() < 2) return eager(s);
+  // a caller that is itself capturing a graph gets plain launches
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return eager(s);
+  }
+  Plan::GraphEntry* e = nullptr;
+  for (auto& g : plan->graphs)
+    if (g.src == src && g.dst == dst && g.dir == direction && g.scale == scale) e = &g;
+  if (!e) {
+    if (plan->graphs.size() >= 8) {  // evict the least recently used
+      auto lru = std::min_element(plan->graphs.begin(), plan->graphs.end(),
+                                  [](const Plan::GraphEntry& x, const Plan::GraphEntry& y) { return x.last < y.last; });
+      if (lru->exec) cudaGraphExecDestroy(lru->exec);
+      plan->graphs.erase(lru);
+    }
+    plan->graphs.push_back(Plan::GraphEntry{src, dst, direction, scale, 0, nullptr, 0});
+    e = &plan->graphs.back();
+  }
+  e->last = ++plan->graph_clock;
+  if (e->exec) {
+    const cudaError_t r = cudaGraphLaunch(e->exec, s);
+    if (r == cudaSuccess) return 0;
+    cudaGetLastError();
+    plan->graphs_off = true;
+    return eager(s);
+  }
+  if (++e->calls < 2) return eager(s);
+  // second call: capture the launch sequence once, then replay it on s
+  if (!plan->capture_stream &&
+      cudaStreamCreateWithFlags(&plan->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    plan->graphs_off = true;
+    return eager(s);
+  }
+  cudaGraph_t graph = nullptr;
+  int rc = 0;
+  bool ok = cudaStreamBeginCapture(plan->capture_stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    rc = eager(plan->capture_stream);
+    ok = cudaStreamEndCapture(plan->capture_stream, &graph) == cudaSuccess && rc == 0 && graph;
+  }
+  if (ok) ok = cudaGraphInstantiate(&e->exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (!ok) {
+    cudaGetLastError();
+    e->exec = nullptr;
+    plan->graphs_off = true;
+    return eager(s);
+  }
+  if (cudaGraphLaunch(e->exec, s) != cudaSuccess) {
+    cudaGetLastError();
+    plan->graphs_off = true;
+    return eager(s);
+  }
+  return 0;
 }
 
 int shafft_sm100_execute_step(shafft_sm100_plan plan, int step, void* src, void* dst, int direction,
