@@ -106,10 +106,15 @@ int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direc
 /* data[i] *= factor over count complex elements (stand-alone normalize). */
 int shafft_sm100_scale(void* data, size_t count, int precision, double factor, void* stream);
 
-/* Status of the plan's last executes: reads the device-side error flag of
- * the fused plane pass (set if one of its bounded waits gave up).  Call after
+/* Status of the plan's last executes: reads the device-side error flags of
+ * the passes with bounded waits (tensor-core passes, bulk-copy column passes,
+ * the fused plane pass), set if one of those waits gave up.  Call after
  * synchronising the stream; returns 0 or SHAFFT_SM100_ECUDA. */
 int shafft_sm100_plan_status(shafft_sm100_plan plan);
+
+/* Column passes launched in this process through the bulk-tensor-copy
+ * kernel (length 256 / 512 column tiles; opt-in with SHAFFT_SM100_TMA=1). */
+int64_t shafft_sm100_tma_launch_count(void);
 
 /* Number of complex elements of the transform. */
 int64_t shafft_sm100_plan_elements(shafft_sm100_plan plan);

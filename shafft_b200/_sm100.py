@@ -66,6 +66,8 @@ def load():
     lib.shafft_sm100_batch_bytes.restype = ctypes.c_int64
     lib.shafft_sm100_batch_describe.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     lib.shafft_sm100_plan_status.argtypes = [vp]
+    lib.shafft_sm100_tma_launch_count.argtypes = []
+    lib.shafft_sm100_tma_launch_count.restype = ctypes.c_int64
     lib.shafft_sm100_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_size_t, ctypes.c_int]
     lib.shafft_sm100_server_submit.argtypes = [vp, ctypes.c_int, i64p, ctypes.c_int, ctypes.c_int,
                                                ctypes.c_double, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
@@ -159,6 +161,11 @@ class Plan:
             self.destroy()
         except Exception:
             pass
+
+
+def tma_launch_count() -> int:
+    """Column passes this process ran through the bulk-tensor-copy kernel."""
+    return int(load().shafft_sm100_tma_launch_count())
 
 
 def scale(ptr: int, count: int, precision: int, factor: float, stream: int = 0):

@@ -61,6 +61,14 @@ struct Chunk {
 };
 
 __device__ __forceinline__ int swz(int p, int c) { return p * 8 + (c ^ (p & 7)); }
+// Layout of a tile whose phase A reads it from shared memory (a bulk tensor
+// copy put it there as dense 128-byte rows): no XOR swizzle.  In a column
+// tile every phase has 8 lanes on the 8 chunks of one row, so it is free of
+// bank conflicts too.
+template <bool SW>
+__device__ __forceinline__ int sidx(int p, int c) {
+  return SW ? swz(p, c) : p * 8 + c;
+}
 
 // Streaming (evict-first) global accesses for the tensor, so that the small
 // twiddle table stays resident in L1; twiddles use the read-only path.
@@ -103,7 +111,10 @@ __device__ __forceinline__ void discard_line(const void* p) {
   asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
 }
 
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_>
+// SMEM_A (column tiles only): the input tile is already in `sm` as dense
+// 128-byte rows (row p = input point p); phase A transforms it in place.
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_,
+          bool SMEM_A = false>
 __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T>::type* in,
                                           typename Cx<T>::type* out,
                                           const PassTables<typename Cx<T>::type>& tb, int64_t tile,
@@ -117,6 +128,8 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
   constexpr int W = 8 * VW;
   constexpr int S = Cfg::S;
   constexpr int RL = (S == 3) ? R2 : R1;  // radix of the last stage
+  constexpr bool SW = !SMEM_A;
+  static_assert(!(SMEM_A && IN_ROW), "shared-memory input is a column tile");
 
   const int tid = threadIdx.x;
   const int64_t tw = tile % g.tiles_w;
@@ -160,6 +173,11 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
           for (int e = 0; e < VW; ++e)
             v[b][r][e] = (LDP == LD_L2) ? ld_l2(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n)
                                         : ld_stream(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n);
+        } else if constexpr (SMEM_A) {
+          float4 raw = sm[n * 8 + bc[b]];
+          const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
+#pragma unroll
+          for (int e = 0; e < VW; ++e) v[b][r][e] = ch.v[e];
         } else {
           const void* src = in + bin + bc[b] * VW + (int64_t)n * g.sn_in;
           float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
@@ -193,7 +211,7 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
 #pragma unroll
         for (int e = 0; e < VW; ++e) ch.v[e] = v[b][r][e];
         const int p = bj[b] + r * M0;
-        sm[swz(p, bc[b])] = *reinterpret_cast<float4*>(&ch);
+        sm[sidx<SW>(p, bc[b])] = *reinterpret_cast<float4*>(&ch);
       }
     }
   }
@@ -225,7 +243,7 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
       C x[R1][VW];
 #pragma unroll
       for (int r = 0; r < R1; ++r) {
-        float4 raw = sm[swz(base + r * M1, c)];
+        float4 raw = sm[sidx<SW>(base + r * M1, c)];
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
         for (int e = 0; e < VW; ++e) x[r][e] = ch.v[e];
@@ -248,7 +266,7 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
         Chunk<C, VW> ch;
 #pragma unroll
         for (int e = 0; e < VW; ++e) ch.v[e] = x[r][e];
-        sm[swz(base + r * M1, c)] = *reinterpret_cast<float4*>(&ch);
+        sm[sidx<SW>(base + r * M1, c)] = *reinterpret_cast<float4*>(&ch);
       }
     }
     __syncthreads();
@@ -275,7 +293,7 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
       C x[RL][VW];
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
-        float4 raw = sm[swz(blk * RL + r, c)];
+        float4 raw = sm[sidx<SW>(blk * RL + r, c)];
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
         for (int e = 0; e < VW; ++e) x[r][e] = ch.v[e];

@@ -13,6 +13,10 @@ namespace shafft_sm100 {
 // shafft_sm100_last_error_message) and return `code`.
 int report_error(int code, const char* msg);
 
+// Launches of the bulk-tensor-copy column pass (k_fft_fast_tma) in this
+// process (plan.cu).
+void count_tma_launch();
+
 // Tensor-core (tcgen05, split FP16) pass for complex64: one DFT stage of
 // length 2..64 over every row of the geometry g (tc.cu).  `err` is a device
 // int set to 1 when a wait for the tensor core gives up.
@@ -48,8 +52,10 @@ struct Launch {
   // specialised pass for a hot length; tile width is 16 bytes x 8 (= 8*VW
   // elements), output is a column tile.  Returns cudaErrorNotSupported when
   // no specialisation exists for L.
+  // Column tiles of L = 256 / 512 go through the bulk-tensor-copy kernel
+  // (k_fft_fast_tma) when the input qualifies; `err` is its device error word.
   static cudaError_t fast(const PassGeom& g, bool in_row, const C* in, C* out,
-                          const PassTables<C>& tb, cudaStream_t s);
+                          const PassTables<C>& tb, int* err, cudaStream_t s);
   static bool fast_supported(int L);
   static int fast_threads(int L);
   // fused two-axis pass over a stack of square L x L planes (see
@@ -91,10 +97,10 @@ cudaError_t Launch<double>::plane(const PassGeom& gx, const PassGeom& gy, const 
                                   int planes, int* ctl, int lag, cudaStream_t s);
 template <>
 cudaError_t Launch<float>::fast(const PassGeom& g, bool in_row, const float2* in, float2* out,
-                                const PassTables<float2>& tb, cudaStream_t s);
+                                const PassTables<float2>& tb, int* err, cudaStream_t s);
 template <>
 cudaError_t Launch<double>::fast(const PassGeom& g, bool in_row, const double2* in, double2* out,
-                                 const PassTables<double2>& tb, cudaStream_t s);
+                                 const PassTables<double2>& tb, int* err, cudaStream_t s);
 
 extern template struct Launch<float>;
 extern template struct Launch<double>;

@@ -6,7 +6,10 @@
 
 #include <algorithm>
 
+#include <cudaTypedefs.h>
+
 #include "fast.cuh"
+#include "fast_tma.cuh"
 #include "kernels.cuh"
 #include "launch.h"
 
@@ -34,6 +37,114 @@ static inline unsigned ew_grid(int64_t n) {
   X(128, 8, 4, 4, 128)          \
   X(256, 8, 8, 4, 128)          \
   X(512, 8, 8, 8, 256)
+
+// Column-tile passes fed by bulk tensor copies (k_fft_fast_tma):
+// (L, R0, R1, R2, threads, stages, CTAs per SM).  Shared memory per CTA is
+// stages x L x 128 bytes (3 x 64 KiB for L = 512: one CTA of 16 warps per SM;
+// 3 x 32 KiB for L = 256: two CTAs of 8 warps).
+#define SHAFFT_TMA_LIST(X)        \
+  X(256, 8, 8, 4, 256, 3, 2)      \
+  X(512, 8, 8, 8, 512, 3, 1)
+
+// SHAFFT_SM100_TMA=1 turns the bulk-copy column passes on (default: the
+// register-load k_fft_fast, which measured faster on B200: 512^3 complex64
+// column pass 0.464 vs 0.534 ms, 2^24 complex64 FFT1D 0.418 vs 0.592 ms
+// fwd+bwd; one CTA per SM cannot overlap its own barriers and butterflies
+// the way three independent CTAs do).  SHAFFT_SM100_TMA_L2 = 0..3 picks the
+// L2 promotion of the copies (none, 64, 128, 256 bytes; default 2; no
+// measurable difference).
+static bool tma_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("SHAFFT_SM100_TMA");
+    return e && atoi(e) != 0;
+  }();
+  return on;
+}
+
+static int tma_l2_promotion() {
+  static const int v = [] {
+    const char* e = getenv("SHAFFT_SM100_TMA_L2");
+    const int x = e ? atoi(e) : 2;
+    return (x >= 0 && x <= 3) ? x : 2;
+  }();
+  return v;
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// Tensor map of a column pass's input (see fast_tma.cuh).  False when the
+// view does not qualify (alignment, strides, extents); the caller then runs
+// the register-load kernel.
+static bool tma_map_for(const PassGeom& g, const void* in, int csize, CUtensorMap* map, TmaDims* d) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tma_encoder();
+  if (!enc || (reinterpret_cast<uintptr_t>(in) & 15) || g.sin[0] != 1) return false;
+  const int box_n = g.L < 256 ? g.L : 256;
+  if (g.L % box_n) return false;
+  // (index, extent, byte stride) of n, b1, b2, b3
+  struct Ax {
+    int id;
+    int64_t ext, stride;
+  } ax[4] = {{0, g.L, g.sn_in * csize}, {1, g.ext[1], g.sin[1] * csize}, {2, g.ext[2], g.sin[2] * csize},
+             {3, g.ext[3], g.sin[3] * csize}};
+  int64_t top = 16;
+  for (const Ax& a : ax) {
+    if (a.ext < 1 || a.ext > (int64_t)1 << 31) return false;
+    if (a.ext > 1) {
+      if (a.stride <= 0 || a.stride % 16) return false;
+      top = std::max(top, a.stride * a.ext);
+    }
+  }
+  // unit axes get a stride past every used one, so that strides ascend
+  for (Ax& a : ax)
+    if (a.ext == 1) a.stride = top;
+  if (top >= (int64_t)1 << 40) return false;
+  std::stable_sort(ax, ax + 4, [](const Ax& x, const Ax& y) { return x.stride < y.stride; });
+  cuuint64_t dims[5], strides[4];
+  cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+  dims[0] = (cuuint64_t)g.ext[0] * (csize / 4);
+  box[0] = 32;
+  if (dims[0] % 32 || dims[0] > ((cuuint64_t)1 << 32)) return false;
+  int pos[4];
+  for (int i = 0; i < 4; ++i) {
+    dims[i + 1] = (cuuint64_t)ax[i].ext;
+    strides[i] = (cuuint64_t)ax[i].stride;
+    box[i + 1] = ax[i].id == 0 ? (cuuint32_t)box_n : 1u;
+    pos[ax[i].id] = i + 1;
+  }
+  d->n = pos[0];
+  d->b1 = pos[1];
+  d->b2 = pos[2];
+  d->b3 = pos[3];
+  const CUtensorMapL2promotion l2[4] = {CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_64B,
+                                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<void*>(in), dims, strides, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         l2[tma_l2_promotion()], CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+static unsigned sm_count() {
+  static const unsigned n = [] {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (unsigned)std::max(1, sms);
+  }();
+  return n;
+}
 
 // Lengths with a fused two-axis plane kernel (k_fft_plane_flow).
 #define SHAFFT_PLANE_LIST_F32(X) \
@@ -93,6 +204,7 @@ static cudaError_t launch_flow(KernelT kernel, int threads, size_t smem, const P
     cudaError_t e = cudaSuccess;                                                                 \
     FASTLIST(SHAFFT_ATTR_FAST)                                                                   \
     PLANELIST(SHAFFT_ATTR_PLANE)                                                                 \
+    SHAFFT_TMA_LIST(SHAFFT_ATTR_TMA)                                                             \
     return e;                                                                                    \
   }                                                                                              \
   template <>                                                                                    \
@@ -118,8 +230,16 @@ static cudaError_t launch_flow(KernelT kernel, int threads, size_t smem, const P
   }                                                                                              \
   template <>                                                                                    \
   cudaError_t Launch<TYPE>::fast(const PassGeom& g, bool in_row, const C* in, C* out,            \
-                                 const PassTables<C>& tb, cudaStream_t s) {                      \
+                                 const PassTables<C>& tb, int* err, cudaStream_t s) {            \
     const unsigned grid = (unsigned)g.ntiles;                                                    \
+    if (!in_row && err && tma_enabled()) {                                                       \
+      CUtensorMap map;                                                                           \
+      TmaDims d;                                                                                 \
+      switch (g.L) {                                                                             \
+        SHAFFT_TMA_LIST(SHAFFT_CASE_TMA)                                                         \
+        default: break;                                                                          \
+      }                                                                                          \
+    }                                                                                            \
     switch (g.L) {                                                                               \
       FASTLIST(SHAFFT_CASE_FAST)                                                                 \
       default: return cudaErrorNotSupported;                                                     \
@@ -152,6 +272,24 @@ static cudaError_t fast_attr_all();
   if (e == cudaSuccess)                                                                           \
     e = cudaFuncSetAttribute(k_fft_plane_flow<TYPE_, L, A, B, C_, NT>,                            \
                              cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+#define SHAFFT_TMA_SMEM(L_, ST) ((size_t)(ST) * (L_) * 128 + 8 * (ST))
+#define SHAFFT_ATTR_TMA(L_, A, B, C_, NT, ST, MB)                                                 \
+  if (e == cudaSuccess)                                                                           \
+    e = cudaFuncSetAttribute(k_fft_fast_tma<TYPE_, L_, A, B, C_, NT, ST, MB>,                         \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, SHAFFT_TMA_SMEM(L_, ST)); \
+  if (e == cudaSuccess)                                                                           \
+    e = cudaFuncSetAttribute(k_fft_fast_tma<TYPE_, L_, A, B, C_, NT, ST, MB>,                         \
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+#define SHAFFT_CASE_TMA(L_, A, B, C_, NT, ST, MB)                                                 \
+  case L_:                                                                                        \
+    if (tma_map_for(g, in, (int)sizeof(C), &map, &d)) {                                           \
+      const unsigned tg = (unsigned)std::min<int64_t>(g.ntiles, (int64_t)sm_count() * (MB));      \
+      k_fft_fast_tma<TYPE_, L_, A, B, C_, NT, ST, MB><<<tg, NT, SHAFFT_TMA_SMEM(L_, ST), s>>>(          \
+          map, g, d, out, tb, err);                                                               \
+      count_tma_launch();                                                                         \
+      return cudaGetLastError();                                                                  \
+    }                                                                                             \
+    break;
 #define SHAFFT_CASE_TRUE(L_, A, B, C_, NT) \
   case L_:                                 \
     return true;

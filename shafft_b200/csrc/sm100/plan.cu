@@ -31,6 +31,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <atomic>
 #include <functional>
 #include <map>
 #include <memory>
@@ -187,7 +188,9 @@ struct Planner {
     tc_mode = prec != 0 ? 0
               : (flags & SHAFFT_SM100_PLAN_TENSOR_CORE) ? 1
               : (flags & SHAFFT_SM100_PLAN_TC_PRIME_AXES) ? 2 : 0;
-    if (tc_mode) off_tcerr = alloc(16);
+    // device error word of passes with bounded waits (tensor-core and
+    // bulk-copy column passes); 0 = ok
+    off_tcerr = alloc(16);
     if (const char* e = getenv("SHAFFT_SM100_PLANE")) plane_enabled = atoi(e) != 0;
     if (const char* e = getenv("SHAFFT_SM100_FLOW_LAG")) flow_lag = std::max(1, atoi(e));
     if (const char* e = getenv("SHAFFT_SM100_ROTATE")) rotate_enabled = atoi(e) != 0;
@@ -898,7 +901,8 @@ struct shafft_sm100_plan_s {
   cudaStream_t stream = nullptr;
   int device = 0;
   int flags = 0;
-  size_t off_tcerr = 0;  // tensor-core passes: device error word (0 = ok)
+  size_t off_tcerr = 0;  // device error word of passes with bounded waits (0 = ok)
+  bool check_err = false;  // some pass may set it (tensor-core or column passes)
   // Replayed launch sequences: executes with the same (src, dst, direction,
   // scale) run as one CUDA graph from the third call on (the first runs
   // eagerly, the second is captured on a private stream).
@@ -982,7 +986,8 @@ struct Launcher {
     }
     if (st.fast)
       return check(K::fast(g, st.fast_row != 0, reinterpret_cast<const C*>(in),
-                           reinterpret_cast<C*>(out), tables(p, st), s),
+                           reinterpret_cast<C*>(out), tables(p, st),
+                           reinterpret_cast<int*>(p->d_tables + p->off_tcerr), s),
                    "fast fft pass");
     return check(K::pass(g, reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), tables(p, st),
                          st.smem, s),
@@ -1196,6 +1201,12 @@ int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int preci
   int rc = pl.plan_nd(p->steps, ndim, dims);
   if (rc) return rc;
   p->off_tcerr = pl.off_tcerr;
+  p->check_err = (flags & (SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES)) != 0;
+  for (const Step& st : p->steps)
+    if (st.fast && !st.fast_row) p->check_err = true;
+  for (const BTable& bt : p->btabs)
+    for (const Step& st : bt.hsteps)
+      if (st.fast && !st.fast_row) p->check_err = true;
   p->ltabs = pl.ltabs;
   p->ntabs = pl.ntabs;
   p->btabs = pl.btabs;
@@ -1406,6 +1417,11 @@ int validate_dims(int ndim, const int64_t* dims, int precision, int64_t* total) 
 
 }  // namespace
 
+namespace shafft_sm100 {
+static std::atomic<int64_t> g_tma_launches{0};
+void count_tma_launch() { g_tma_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace shafft_sm100
+
 extern "C" {
 
 int shafft_sm100_plan_query(int ndim, const int64_t* dims, int precision, char* buf, int buflen) {
@@ -1613,13 +1629,16 @@ int shafft_sm100_scale(void* data, size_t count, int precision, double factor, v
   return 0;
 }
 
+int64_t shafft_sm100_tma_launch_count(void) { return shafft_sm100::g_tma_launches.load(); }
+
 int shafft_sm100_plan_status(shafft_sm100_plan plan) {
   if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
-  if (plan->flags & (SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES)) {
+  if (plan->check_err) {
     int flag = 0;
     CUDA_TRY(cudaMemcpy(&flag, plan->d_tables + plan->off_tcerr, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag)
-      return set_err(SHAFFT_SM100_ECUDA, "tensor-core pass: a wait for the MMA results timed out");
+      return set_err(SHAFFT_SM100_ECUDA,
+                     "a pass gave up waiting (tensor-core MMA results or a bulk tensor copy)");
   }
   for (const Step& st : plan->steps) {
     if (st.kind != ST_PLANE) continue;
