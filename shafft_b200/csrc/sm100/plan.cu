@@ -1202,11 +1202,15 @@ int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int preci
   if (rc) return rc;
   p->off_tcerr = pl.off_tcerr;
   p->check_err = (flags & (SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES)) != 0;
-  for (const Step& st : p->steps)
-    if (st.fast && !st.fast_row) p->check_err = true;
-  for (const BTable& bt : p->btabs)
-    for (const Step& st : bt.hsteps)
+  // column passes can set it only through the opt-in bulk-copy kernel
+  const char* tma = getenv("SHAFFT_SM100_TMA");
+  if (tma && atoi(tma) != 0) {
+    for (const Step& st : p->steps)
       if (st.fast && !st.fast_row) p->check_err = true;
+    for (const BTable& bt : p->btabs)
+      for (const Step& st : bt.hsteps)
+        if (st.fast && !st.fast_row) p->check_err = true;
+  }
   p->ltabs = pl.ltabs;
   p->ntabs = pl.ntabs;
   p->btabs = pl.btabs;
