@@ -78,10 +78,14 @@ def build(verbose: bool = False, jobs: int = 8) -> dict:
     shim_o = os.path.join(OBJ, "mpi_shim.o")
     if _newer(shim_o, [shim_src] + host_hdrs):
         jobs_list.append([CXX] + CXXFLAGS + ["-c", shim_src, "-o", shim_o])
-    host_src = os.path.join(host, "shafft_host.cpp")
-    host_o = os.path.join(OBJ, "shafft_host.o")
-    if _newer(host_o, [host_src] + host_hdrs):
-        jobs_list.append([CXX] + CXXFLAGS + ["-c", host_src, "-o", host_o])
+    # the C++ API + C ABI, and the Fortran binding's entry points
+    host_objs = []
+    for name in ("shafft_host", "shafft_f03"):
+        src = os.path.join(host, name + ".cpp")
+        o = os.path.join(OBJ, name + ".o")
+        host_objs.append(o)
+        if _newer(o, [src] + host_hdrs):
+            jobs_list.append([CXX] + CXXFLAGS + ["-c", src, "-o", o])
 
     out = []
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
@@ -99,8 +103,8 @@ def build(verbose: bool = False, jobs: int = 8) -> dict:
         out.append(_run([CXX, "-shared", "-o", shim_lib, shim_o]))
     libs["mpishim"] = shim_lib
     host_lib = os.path.join(LIB, "libshafft.so")
-    if _newer(host_lib, [host_o, sm_lib, shim_lib]):
-        out.append(_run([CXX, "-shared", "-o", host_lib, host_o, "-L", LIB, "-lshafft_sm100",
+    if _newer(host_lib, host_objs + [sm_lib, shim_lib]):
+        out.append(_run([CXX, "-shared", "-o", host_lib] + host_objs + ["-L", LIB, "-lshafft_sm100",
                          "-lshafft_mpishim", "-Wl,-rpath,$ORIGIN"]))
     libs["shafft"] = host_lib
     if verbose:

@@ -196,9 +196,11 @@ public:
     return ok();
   }
 
+  // valid from init on: the plan holds its communicator from configure
+  // (src/cpp/detail/plan_data_base.hpp:82-83; src/cpp/shafft.cpp:877-892)
   int communicator(MPI_Comm* out) const {
     if (!out) return fail(SHAFFT_ERR_NULLPTR);
-    if (!planned) return fail(SHAFFT_ERR_PLAN_NOT_INIT);
+    if (!configured) return fail(SHAFFT_ERR_PLAN_NOT_INIT);
     if (!active || comm == MPI_COMM_NULL) {
       *out = MPI_COMM_NULL;
       return ok();

@@ -32,6 +32,7 @@ def declared_functions(header):
 
 @pytest.mark.parametrize("header,lib", [
     ("include/shafft/shafft.h", "shafft_b200/lib/libshafft.so"),
+    ("include/shafft/shafft_f03.h", "shafft_b200/lib/libshafft.so"),
     ("include/shafft_sm100.h", "shafft_b200/lib/libshafft_sm100.so"),
     ("include/mpi_shim/mpi.h", "shafft_b200/lib/libshafft_mpishim.so"),
 ])
