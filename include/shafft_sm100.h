@@ -219,6 +219,25 @@ int shafft_sm100_unpack_blocks(const void* src, void* dst, int64_t outer, int64_
 int shafft_sm100_twiddle_rows(void* data, int64_t rows, int64_t cols, int64_t col0, int64_t N,
                               int sign, int precision, void* stream);
 
+/* Distributed Bluestein (FFT1D lengths not divisible by P^2; replaces the
+ * reference's computeLocalChirpB / computeLocalConvolutionChirp,
+ * 1d/fft1d_bluestein_executor.hip:150-198).  For i < count:
+ *   b[i] = exp(-i*pi*n^2/N) at n = n0 + i < N, else 0
+ *   v[i] = conj(b[m]) for m < N, conj(b[M-m]) for M-N < m < M, else 0, at
+ *          m = m0 + i
+ * (n^2 reduced mod 2N in integers, FP64 sincospi).  Either of b, v may be
+ * NULL; M >= 2N - 1. */
+int shafft_sm100_bluestein_chirps(void* b, void* v, int64_t N, int64_t M, int64_t n0, int64_t m0,
+                                  int64_t count, int precision, void* stream);
+
+/* dst[i] = conj_out(conj_in(src[i]) * factors[i] * scale) for i < valid and
+ * 0 for valid <= i < count (src may equal dst): Bluestein's modulate,
+ * spectrum-multiply and scale+demodulate steps (reference
+ * 1d/fft1d_bluestein_executor.hip:38-129). */
+int shafft_sm100_chirp_multiply(const void* src, void* dst, const void* factors, int64_t count,
+                                int64_t valid, int conj_in, int conj_out, double scale, int precision,
+                                void* stream);
+
 /* Device memory and stream helpers, so that callers above this ABI need no
  * CUDA runtime of their own (they replace the reference's allocBufferT /
  * freeBufferT / copyToBufferT / copyFromBufferT,

@@ -120,10 +120,116 @@ int twiddle_rows(void* data, int64_t rows, int64_t cols, int64_t col0, int64_t N
   return e == cudaSuccess ? 0 : report_error(SHAFFT_SM100_ECUDA, cudaGetErrorString(e));
 }
 
+// Distributed Bluestein (the reference's path B for FFT1D lengths not
+// divisible by P^2, src/cpp/fft/hipfft_method/1d/fft1d_bluestein_executor.hip):
+// each rank holds the M/P-element block of the length-M convolution that
+// starts at its N-space offset, so the chirps are generated per block.
+//   b[i] = exp(-i pi n^2 / N) at n = n0 + i < N, else 0       (:150-166)
+//   v[i] = conj(b[m]) for m < N, conj(b[M - m]) for M - N < m < M,
+//          else 0, at m = m0 + i                                 (:168-198)
+// with n^2 reduced modulo 2N in integers before the FP64 sincospi, so the
+// phase is exact for every N < 2^31.
+template <typename C, typename T>
+__device__ __forceinline__ C chirp_at(int64_t n, int64_t N, double sign) {
+  const uint64_t r = (uint64_t)(((unsigned __int128)(uint64_t)n * (uint64_t)n) % (unsigned __int128)(2 * N));
+  double sn, cs;
+  sincospi(sign * ((double)r / (double)N), &sn, &cs);
+  return C{(T)cs, (T)sn};
+}
+
+template <typename C, typename T>
+__global__ void k_bluestein_chirps(C* b, C* v, int64_t N, int64_t M, int64_t n0, int64_t m0, int64_t count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (b) {
+      const int64_t n = n0 + i;
+      b[i] = n < N ? chirp_at<C, T>(n, N, -1.0) : C{0, 0};
+    }
+    if (v) {
+      const int64_t m = m0 + i;
+      const int64_t j = m < N ? m : (m > M - N && m < M ? M - m : -1);
+      v[i] = j >= 0 ? chirp_at<C, T>(j, N, 1.0) : C{0, 0};
+    }
+  }
+}
+
+// dst[i] = conj_out(conj_in(src[i]) * f[i] * scale) for i < valid, 0 for
+// valid <= i < count: the modulate, spectrum-multiply and scale+demodulate
+// steps of Bluestein (the reference's :38-129 kernels, scale folded in).
+template <typename C, typename T>
+__global__ void k_chirp_multiply(const C* src, C* dst, const C* f, int64_t count, int64_t valid, int conj_in,
+                                 int conj_out, T scale) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    C y{0, 0};
+    if (i < valid) {
+      C a = src[i];
+      if (conj_in) a.y = -a.y;
+      const C w = f[i];
+      y = C{(a.x * w.x - a.y * w.y) * scale, (a.x * w.y + a.y * w.x) * scale};
+      if (conj_out) y.y = -y.y;
+    }
+    dst[i] = y;
+  }
+}
+
+unsigned ew_blocks(int64_t total) {
+  const int64_t want = (total + 255) / 256;
+  return (unsigned)(want < 148 * 16 ? want : 148 * 16);
+}
+
+int bluestein_chirps(void* b, void* v, int64_t N, int64_t M, int64_t n0, int64_t m0, int64_t count,
+                     int precision, void* stream) {
+  if ((!b && !v) || N < 1 || M < 2 * N - 1 || n0 < 0 || m0 < 0 || count < 0 ||
+      (precision != 0 && precision != 1) || N > ((int64_t)1 << 40))
+    return report_error(SHAFFT_SM100_EINVAL, "bluestein chirps: bad arguments");
+  if (count == 0) return 0;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision)
+    k_bluestein_chirps<double2, double><<<ew_blocks(count), 256, 0, s>>>(
+        static_cast<double2*>(b), static_cast<double2*>(v), N, M, n0, m0, count);
+  else
+    k_bluestein_chirps<float2, float><<<ew_blocks(count), 256, 0, s>>>(
+        static_cast<float2*>(b), static_cast<float2*>(v), N, M, n0, m0, count);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : report_error(SHAFFT_SM100_ECUDA, cudaGetErrorString(e));
+}
+
+int chirp_multiply(const void* src, void* dst, const void* f, int64_t count, int64_t valid, int conj_in,
+                   int conj_out, double scale, int precision, void* stream) {
+  if (!src || !dst || !f || count < 0 || valid < 0 || (precision != 0 && precision != 1))
+    return report_error(SHAFFT_SM100_EINVAL, "chirp multiply: bad arguments");
+  if (count == 0) return 0;
+  if (valid > count) valid = count;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision)
+    k_chirp_multiply<double2, double><<<ew_blocks(count), 256, 0, s>>>(
+        static_cast<const double2*>(src), static_cast<double2*>(dst), static_cast<const double2*>(f), count,
+        valid, conj_in, conj_out, scale);
+  else
+    k_chirp_multiply<float2, float><<<ew_blocks(count), 256, 0, s>>>(
+        static_cast<const float2*>(src), static_cast<float2*>(dst), static_cast<const float2*>(f), count,
+        valid, conj_in, conj_out, (float)scale);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : report_error(SHAFFT_SM100_ECUDA, cudaGetErrorString(e));
+}
+
 }  // namespace
 }  // namespace shafft_sm100
 
 extern "C" {
+
+int shafft_sm100_bluestein_chirps(void* b, void* v, int64_t N, int64_t M, int64_t n0, int64_t m0,
+                                  int64_t count, int precision, void* stream) {
+  return shafft_sm100::bluestein_chirps(b, v, N, M, n0, m0, count, precision, stream);
+}
+
+int shafft_sm100_chirp_multiply(const void* src, void* dst, const void* factors, int64_t count,
+                                int64_t valid, int conj_in, int conj_out, double scale, int precision,
+                                void* stream) {
+  return shafft_sm100::chirp_multiply(src, dst, factors, count, valid, conj_in, conj_out, scale,
+                                      precision, stream);
+}
 
 int shafft_sm100_twiddle_rows(void* data, int64_t rows, int64_t cols, int64_t col0, int64_t N,
                               int sign, int precision, void* stream) {

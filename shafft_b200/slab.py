@@ -26,7 +26,8 @@ longer, detail/partition.hpp:40-44), buffer-swap contract (the result is in
 the buffer get_buffers() reports as data) and (1/sqrt(N))^k normalisation.
 Methods return the reference's status codes.  Ranks beyond prod(commDims)
 are inactive: they own no data and belong to no grid line.  FFT1D (below) is
-the reference's distributed 1-D transform (the P x P four-step path).
+the reference's distributed 1-D transform (the P x P four-step path, and
+Bluestein over it for lengths P^2 does not divide).
 """
 from __future__ import annotations
 
@@ -513,25 +514,74 @@ class FFTND:
         return 0
 
 
+def select_path_1d(n: int, nranks: int):
+    """(path, fft_length, local_size) of a distributed 1-D transform of n
+    points on nranks ranks: the reference's selectPath with its default
+    padding rule (src/cpp/fft/hipfft_method/1d/fft1d_path_selector.hpp:30-107,
+    fft1d_handle.hpp:16-22, padding not allowed).  The P x P four-step runs
+    when P^2 divides n; otherwise Bluestein, whose convolution length M is
+    2n - 1 rounded up to a multiple of P^2."""
+    p2 = nranks * nranks
+    if n % p2 == 0:
+        return "cooley_tukey", n, n // nranks
+    m = -(-(2 * n - 1) // p2) * p2
+    return "bluestein", m, m // nranks
+
+
+def _block_1d(n: int, size: int, rank: int):
+    """(local_n, local_start) of rank in blocks of `size` over n points, the
+    start clamped to n (fft1d_method.hip:96-106)."""
+    off = rank * size
+    return (min(size, n - off) if off < n else 0), min(off, n)
+
+
+def configuration_1d(n: int, world: int, rank: int):
+    """(local_n, local_start, local_alloc, active_ranks): the reference's
+    fft1dQueryLayout (fft1d_method.hip:329-414).  The path chosen for all
+    `world` ranks gives the block size; ranks whose block is empty are
+    inactive (all zeros); the path is then chosen again for the active ranks
+    0 .. active_ranks-1, whose blocks (input and output alike) follow."""
+    _, _, l0 = select_path_1d(n, world)
+    active = min(world, -(-n // l0))
+    if rank * l0 >= n:
+        return 0, 0, 0, active
+    _, _, l = select_path_1d(n, active)
+    ln, ls = _block_1d(n, l, rank)
+    return ln, ls, l, active
+
+
 class FFT1D:
-    """Distributed shafft::FFT1D over a torch.distributed group: the
-    reference's P x P four-step path (src/cpp/fft/hipfft_method/1d/
-    fft1d_cooley_tukey_executor.hip:175-290), for N divisible by P^2.  Rank r
-    holds the contiguous block x[r*L, (r+1)*L), L = N/P, before and after a
-    transform.  With C = L/P:
+    """Distributed shafft::FFT1D over a torch.distributed group.  The layout
+    is configuration_1d's: ranks 0 .. A-1 are active and rank r holds
+    x[r*L, r*L + local_n) in a buffer of L elements (the same block before
+    and after a transform); the other ranks are inactive and every call on
+    them returns 0 without work.  The active ranks form their own process
+    group (created by every rank of the group, in the same order).
+
+    Path A (A^2 divides N; src/cpp/fft/hipfft_method/1d/
+    fft1d_cooley_tukey_executor.hip:175-290), the A x A four-step over
+    F = N points with L = F/A and C = L/A:
 
       1. all-to-all of C-element chunks      -> [s][c] = x[s*L + r*C + c]
-      2. length-P DFTs over s (one column pass of a [P][C] plan)
+      2. length-A DFTs over s (one column pass of an [A][C] plan)
                                               -> [k1][c], already the send order
-      3. twiddle w_N^{(r*C + c) k1}           (shafft_sm100_twiddle_rows)
+      3. twiddle w_F^{(r*C + c) k1}           (shafft_sm100_twiddle_rows)
       4. all-to-all                           -> [s][c] = column r*... of k1 = r
-      5. length-L DFT                         -> X[r + P*k2] at k2
-      6. all-to-all of the C-chunks of k2     -> [s][j] = X[r*L + s + P*j]
-      7. [P][C] -> [C][P] transpose           (shafft_sm100_unpack_blocks)
+      5. length-L DFT                         -> X[r + A*k2] at k2
+      6. all-to-all of the C-chunks of k2     -> [s][j] = X[r*L + s + A*j]
+      7. [A][C] -> [C][A] transpose           (shafft_sm100_unpack_blocks)
+
+    Path B (otherwise; 1d/fft1d_bluestein_executor.hip:209-448): Bluestein
+    with the four-step above over the convolution length F = M.  At plan
+    time each rank generates its blocks of the chirp b and of the kernel v
+    (shafft_sm100_bluestein_chirps) and transforms v; an execute modulates
+    (conjugating the input for a backward transform), runs the forward
+    four-step, multiplies by the kernel's spectrum, runs the backward
+    four-step, and scales by 1/M while demodulating (conjugating the output
+    for a backward transform) -- all through shafft_sm100_chirp_multiply.
 
     The result is in the buffer get_buffers() reports as data (the buffers
-    swap on every execute, Slab1D::swapBuffers).  Lengths not divisible by
-    P^2 (the reference's distributed Bluestein) return ERR_NOT_IMPL."""
+    swap on every execute, Slab1D::swapBuffers)."""
 
     def __init__(self):
         self._state = "created"
@@ -546,15 +596,24 @@ class FFT1D:
         n, local_n, local_start = int(n), int(local_n), int(local_start)
         if n < 1:
             return ERR_INVALID_DIM
-        P = dist.get_world_size(group) if dist.is_initialized() else 1
+        world = dist.get_world_size(group) if dist.is_initialized() else 1
         r = dist.get_rank(group) if dist.is_initialized() else 0
-        if n % (P * P):
-            return ERR_NOT_IMPL
-        L = n // P
-        if local_n != L or local_start != r * L:
+        ln, ls, la, active = configuration_1d(n, world, r)
+        if (local_n, local_start) != (ln, ls):
             return ERR_INVALID_DECOMP
-        self.N, self.P, self.rank, self.L, self.C = n, P, r, L, L // P
-        self.precision, self.group, self.ops = precision, group, device_ops
+        # the active ranks' group (every rank of `group` takes part)
+        sub = group
+        if world > 1 and active < world:
+            ranks = list(range(active))
+            if group is not None:
+                ranks = [dist.get_global_rank(group, x) for x in ranks]
+            sub = dist.new_group(ranks)
+        self.active = r < active
+        self.N, self.precision, self.ops = n, precision, device_ops
+        self.A, self.rank, self.local_n, self.local_start = active, r, ln, ls
+        self.path, self.F, self.L = select_path_1d(n, active)
+        self.C = self.L // active
+        self.group = sub if self.active else None
         self._state = "configured"
         return 0
 
@@ -563,13 +622,23 @@ class FFT1D:
             return ERR_PLAN_NOT_INIT
         if self._state != "configured":
             return ERR_INVALID_STATE
-        if self.ops is None:
-            self.ops = CudaOps(self.precision)
-        if self.P == 1:
-            self.plans = [self.ops.plan([self.N], [0])]
-        else:
-            self.plans = [self.ops.plan([self.P, self.C], [0]), self.ops.plan([self.L], [0])]
+        self.plans = []
         self.data = self.work = self.scratch = None
+        if self.active:
+            if self.ops is None:
+                self.ops = CudaOps(self.precision)
+            if self.A == 1:
+                self.plans = [self.ops.plan([self.N], [0])]
+            else:
+                self.plans = [self.ops.plan([self.A, self.C], [0]), self.ops.plan([self.L], [0])]
+            if self.path == "bluestein":
+                L, ops = self.L, self.ops
+                self.chirp = ops.empty(L)
+                self.vhat = ops.empty(L)
+                self.mbuf = [ops.empty(L), ops.empty(L), ops.empty(L)]
+                ops.chirps(self.chirp, None, self.N, self.F, self.local_start, self.rank * L, L)
+                ops.chirps(None, self.mbuf[0], self.N, self.F, self.local_start, self.rank * L, L)
+                self._four_step(self.mbuf[0], self.vhat, self.mbuf[1], FORWARD)
         self._state = "planned"
         return 0
 
@@ -577,14 +646,26 @@ class FFT1D:
         for h in getattr(self, "plans", []):
             self.ops.destroy(h)
         self.plans = []
+        self.chirp = self.vhat = None
+        self.mbuf = []
         self._state = "released"
 
     def alloc_size(self) -> int:
-        return self.L if self._state in ("configured", "planned") else 0
+        return self.L if self._state in ("configured", "planned") and self.active else 0
+
+    def get_layout(self):
+        """(status, local_n, local_start): the same block before and after a
+        transform (fft1d_method.hip:396-397)."""
+        if self._state not in ("configured", "planned"):
+            return ERR_PLAN_NOT_INIT, 0, 0
+        return 0, self.local_n, self.local_start
 
     def set_buffers(self, data, work) -> int:
         if self._state != "planned":
             return ERR_PLAN_NOT_INIT
+        if not self.active:  # inactive ranks may pass nothing
+            self.data, self.work = data, work
+            return 0
         if data is None or work is None:
             return ERR_NULLPTR
         if data.numel() < self.L or work.numel() < self.L or data.data_ptr() == work.data_ptr():
@@ -596,26 +677,43 @@ class FFT1D:
     def get_buffers(self):
         return 0, self.data, self.work
 
+    def _four_step(self, x, w, s, direction):
+        """Steps 1-7 of the class docstring over F points; x and s are
+        clobbered, the result lands in w."""
+        ops, A, C = self.ops, self.A, self.C
+        if A == 1:
+            ops.execute(self.plans[0], x, w, direction)
+            return
+        eq = [C] * A
+        ops.alltoall(w, x, eq, eq, self.group, A)                   # 1
+        ops.execute(self.plans[0], w, s, direction)                 # 2  [k1][c]
+        ops.twiddle(s, A, C, self.rank * C, self.F, -1 if direction == FORWARD else 1)  # 3
+        ops.alltoall(x, s, eq, eq, self.group, A)                   # 4
+        ops.execute(self.plans[1], x, s, direction)                 # 5  X[r + A k2]
+        ops.alltoall(x, s, eq, eq, self.group, A)                   # 6  [s][j]
+        ops.unpack(x, w, C, A, 1, A)                                # 7  [j][s]
+
     def execute(self, direction) -> int:
         if self._state != "planned":
             return ERR_PLAN_NOT_INIT
-        if self.data is None:
-            return ERR_NO_BUFFER
         if direction not in (FORWARD, BACKWARD):
             return ERR_INVALID_STATE
-        x, w, s = self.data, self.work, self.scratch
-        if self.P == 1:
-            self.ops.execute(self.plans[0], x, w, direction)
+        if not self.active:
+            self.norm_exponent += 1
+            return 0
+        if self.data is None:
+            return ERR_NO_BUFFER
+        x, w = self.data, self.work
+        if self.path == "cooley_tukey":
+            self._four_step(x, w, self.scratch, direction)
         else:
-            P, C, L = self.P, self.C, self.L
-            eq = [C] * P
-            self.ops.alltoall(w, x, eq, eq, self.group, P)              # 1
-            self.ops.execute(self.plans[0], w, s, direction)            # 2  [k1][c]
-            self.ops.twiddle(s, P, C, self.rank * C, self.N, -1 if direction == FORWARD else 1)  # 3
-            self.ops.alltoall(x, s, eq, eq, self.group, P)              # 4
-            self.ops.execute(self.plans[1], x, s, direction)            # 5  X[r + P k2]
-            self.ops.alltoall(x, s, eq, eq, self.group, P)              # 6  [s][j]
-            self.ops.unpack(x, w, C, P, 1, P)                           # 7  [j][s]
+            ops, L, (m0, m1, m2) = self.ops, self.L, self.mbuf
+            back = 1 if direction == BACKWARD else 0
+            ops.chirp_mul(x, m0, self.chirp, L, self.local_n, back, 0, 1.0)        # modulate
+            self._four_step(m0, m1, m2, FORWARD)
+            ops.chirp_mul(m1, m1, self.vhat, L, L, 0, 0, 1.0)                      # convolve
+            self._four_step(m1, m0, m2, BACKWARD)
+            ops.chirp_mul(m0, w, self.chirp, L, self.local_n, 0, back, 1.0 / self.F)  # demodulate
         self.data, self.work = w, x
         self.norm_exponent += 1
         return 0
@@ -627,7 +725,7 @@ class FFT1D:
         if self._state != "planned":
             return ERR_PLAN_NOT_INIT
         k = self.norm_exponent
-        if k:
+        if k and self.active:
             if self.precision == C2C:
                 f = float(np.float32(1.0) / np.power(np.sqrt(np.float32(self.N)), np.float32(k)))
             else:
@@ -657,6 +755,12 @@ class CudaOps:
         for f in (self.lib.shafft_sm100_pack_blocks, self.lib.shafft_sm100_unpack_blocks):
             f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
                           ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        self.lib.shafft_sm100_bluestein_chirps.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+            ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p]
+        self.lib.shafft_sm100_chirp_multiply.argtypes = [
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+            ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p]
         self.precision = precision
         self.torch = torch
 
@@ -698,6 +802,22 @@ class CudaOps:
         self._sm._check(self.lib.shafft_sm100_scale(ctypes.c_void_p(data.data_ptr()), count,
                                                     self.precision, ctypes.c_double(factor),
                                                     self._stream()), "scale")
+
+    def empty(self, count):
+        dt = self.torch.complex128 if self.precision == Z2Z else self.torch.complex64
+        return self.torch.empty(count, dtype=dt, device="cuda")
+
+    def chirps(self, b, v, n, m, n0, m0, count):
+        ptr = (lambda t: None if t is None else t.data_ptr())
+        self._sm._check(self.lib.shafft_sm100_bluestein_chirps(ptr(b), ptr(v), n, m, n0, m0, count,
+                                                               self.precision, self._stream()),
+                        "bluestein_chirps")
+
+    def chirp_mul(self, src, dst, factors, count, valid, conj_in, conj_out, scale):
+        self._sm._check(self.lib.shafft_sm100_chirp_multiply(src.data_ptr(), dst.data_ptr(),
+                                                             factors.data_ptr(), count, valid, conj_in,
+                                                             conj_out, scale, self.precision,
+                                                             self._stream()), "chirp_multiply")
 
     def alltoall(self, out, inp, out_counts, in_counts, group, world):
         import torch.distributed as dist

@@ -172,34 +172,40 @@ torch.cuda.set_device(0)
 dist.init_process_group("gloo")
 r, P = dist.get_rank(), dist.get_world_size()
 N, prec = cfg["n"], cfg["prec"]
-L = N // P
+ln, ls, la, active = slab.configuration_1d(N, P, r)
 dt = np.complex128 if prec == S.Z2Z else np.complex64
 g = o.uniform_input((N,), seed=42, dtype=dt)
-ref = o.fftn(g.astype(np.complex128), precise=(prec == S.Z2Z))[r * L:(r + 1) * L]
+ref = o.fftn(g.astype(np.complex128), precise=(prec == S.Z2Z))[ls:ls + ln]
 plan = slab.FFT1D()
-assert plan.init(N, L, r * L, prec) == 0
+assert plan.init(N, ln, ls, prec) == 0
 assert plan.plan() == 0
+path = plan.path if r < active else None
 tdt = torch.complex128 if prec == S.Z2Z else torch.complex64
-a = torch.zeros(L, dtype=tdt, device="cuda"); b = torch.zeros_like(a)
+a = torch.zeros(max(la, 1), dtype=tdt, device="cuda"); b = torch.zeros_like(a)
 assert plan.set_buffers(a, b) == 0
-a.copy_(torch.from_numpy(g[r * L:(r + 1) * L]).cuda())
+a[:ln].copy_(torch.from_numpy(g[ls:ls + ln]).cuda())
 assert plan.execute(S.FORWARD) == 0
 _, d, _ = plan.get_buffers()
-y = d.cpu().numpy()
+y = d[:ln].cpu().numpy()
 err2 = float(np.sum(np.abs(y - ref) ** 2)); ref2 = float(np.sum(np.abs(ref) ** 2))
 assert plan.execute(S.BACKWARD) == 0 and plan.normalize() == 0
 _, d, _ = plan.get_buffers()
-x = g[r * L:(r + 1) * L]
-bt2 = float(np.sum(np.abs(d.cpu().numpy() - x) ** 2)); g2 = float(np.sum(np.abs(x) ** 2))
+x = g[ls:ls + ln]
+bt2 = float(np.sum(np.abs(d[:ln].cpu().numpy() - x) ** 2)); g2 = float(np.sum(np.abs(x) ** 2))
 plan.release()
 dist.destroy_process_group()
-json.dump({"err2": err2, "ref2": ref2, "bt2": bt2, "g2": g2}, open(sys.argv[2], "w"))
+json.dump({"err2": err2, "ref2": ref2, "bt2": bt2, "g2": g2, "ln": ln, "path": path}, open(sys.argv[2], "w"))
 '''
 
 
-@pytest.mark.parametrize("n,prec", [(1 << 20, S.C2C), (121500, S.C2C), (1 << 18, S.Z2Z)])
-def test_distributed_fft1d_two_ranks(tmp_path, n, prec):
-    world = 2
+@pytest.mark.parametrize("world,n,prec,path", [
+    (2, 1 << 20, S.C2C, "cooley_tukey"), (2, 121500, S.C2C, "cooley_tukey"), (2, 1 << 18, S.Z2Z, "cooley_tukey"),
+    (3, 100003, S.C2C, "bluestein"),   # 2 active ranks (M = 200008), the third inactive
+    (6, 100003, S.Z2Z, "bluestein"),   # 3 active ranks (M = 200007), three inactive
+    (3, 1000, S.C2C, "cooley_tukey")])  # one inactive rank, four-step re-chosen for two
+def test_distributed_fft1d(tmp_path, world, n, prec, path):
+    """The reference's distributed FFT1D layout and both paths (four-step,
+    Bluestein over it), every device step on the GPU that the ranks share."""
     script = tmp_path / "worker1d.py"
     script.write_text(WORKER_1D)
     port = _free_port()
@@ -212,7 +218,52 @@ def test_distributed_fft1d_two_ranks(tmp_path, n, prec):
     for p in procs:
         assert p.wait(timeout=300) == 0
     res = [json.loads((tmp_path / f"r{r}.json").read_text()) for r in range(world)]
+    assert sum(x["ln"] for x in res) == n
+    assert res[0]["path"] == path
     err = math.sqrt(sum(x["err2"] for x in res) / sum(x["ref2"] for x in res))
     back = math.sqrt(sum(x["bt2"] for x in res) / sum(x["g2"] for x in res))
     assert err <= tol(n, prec), err
     assert back <= 2 * tol(n, prec), back
+
+
+def _chirp_ref(idx, n, sign):
+    r = np.array([(int(k) * int(k)) % (2 * n) for k in idx], dtype=np.float64)
+    return np.exp(sign * 1j * np.pi * r / n)
+
+
+@pytest.mark.parametrize("prec", [S.C2C, S.Z2Z])
+@pytest.mark.parametrize("n,m,n0,m0,count", [(1001, 2004, 0, 0, 1002), (1001, 2004, 1001, 1002, 1002),
+                                             (100003, 200007, 66669, 66669, 66669),
+                                             ((1 << 31) - 1, 1 << 32, (1 << 31) - 40, (1 << 32) - 44, 64)])
+def test_bluestein_chirp_kernels(prec, n, m, n0, m0, count):
+    """shafft_sm100_bluestein_chirps (exact n^2 mod 2N phases, also near
+    N = 2^31) and shafft_sm100_chirp_multiply against numpy."""
+    from shafft_b200.slab import CudaOps
+    import torch
+    ops = CudaOps(prec)
+    b, v = ops.empty(count), ops.empty(count)
+    ops.chirps(b, v, n, m, n0, m0, count)
+    i = np.arange(count, dtype=np.int64)
+    k = n0 + i
+    b_ref = np.where(k < n, _chirp_ref(np.minimum(k, n - 1), n, -1), 0)
+    mm = m0 + i
+    j = np.where(mm < n, mm, np.where((mm > m - n) & (mm < m), m - mm, -1))
+    v_ref = np.where(j >= 0, _chirp_ref(np.maximum(j, 0), n, 1), 0)
+    t = 2e-7 if prec == S.C2C else 1e-15
+    assert np.abs(b.cpu().numpy() - b_ref).max() <= t
+    assert np.abs(v.cpu().numpy() - v_ref).max() <= t
+    dt = np.complex128 if prec == S.Z2Z else np.complex64
+    x = o.uniform_input((count,), seed=5, dtype=dt)
+    xs = torch.from_numpy(x).cuda()
+    out = ops.empty(count)
+    valid = count * 2 // 3
+    for conj_in, conj_out, scale in ((0, 0, 1.0), (1, 0, 0.5), (0, 1, 1.0 / m), (1, 1, 3.0)):
+        ops.chirp_mul(xs, out, b, count, valid, conj_in, conj_out, scale)
+        a = np.conj(x) if conj_in else x
+        want = a * b.cpu().numpy() * scale
+        want = np.conj(want) if conj_out else want
+        want[valid:] = 0
+        got = out.cpu().numpy()
+        assert np.abs(got - want).max() <= 4 * t * max(1.0, scale), (conj_in, conj_out, scale)
+    ops.chirp_mul(xs, xs, v, count, count, 0, 0, 1.0)  # in place
+    assert np.abs(xs.cpu().numpy() - x * v.cpu().numpy()).max() <= 4 * t

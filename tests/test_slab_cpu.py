@@ -59,30 +59,54 @@ class NumpyOps:
     def alltoall(self, out, inp, oc, ic, group, world):
         o = torch.view_as_real(out[:sum(oc)]).view(-1); i = torch.view_as_real(inp[:sum(ic)]).view(-1)
         dist.all_to_all_single(o, i, [2 * c for c in oc], [2 * c for c in ic], group=group)
+    def empty(self, count): return torch.zeros(count, dtype=torch.complex128)
+    def chirps(self, b, v, n, m, n0, m0, count):
+        def chirp(idx, sign):
+            r = (idx.astype(object) ** 2 % (2 * n)).astype(np.float64)
+            return np.exp(sign * 1j * np.pi * r / n)
+        i = np.arange(count, dtype=np.int64)
+        if b is not None:
+            k = n0 + i
+            b[:count] = torch.from_numpy(np.where(k < n, chirp(np.minimum(k, n - 1), -1), 0))
+        if v is not None:
+            mm = m0 + i
+            j = np.where(mm < n, mm, np.where((mm > m - n) & (mm < m), m - mm, -1))
+            v[:count] = torch.from_numpy(np.where(j >= 0, chirp(np.maximum(j, 0), 1), 0))
+    def chirp_mul(self, src, dst, f, count, valid, conj_in, conj_out, scale):
+        a = src[:count].numpy().copy()
+        if conj_in: a = np.conj(a)
+        y = a * f[:count].numpy() * scale
+        if conj_out: y = np.conj(y)
+        y[valid:] = 0
+        dst[:count] = torch.from_numpy(y)
 
 cfg = json.loads(sys.argv[3])
 dist.init_process_group("gloo")
 rank, world = dist.get_rank(), dist.get_world_size()
 if cfg.get("fft1d"):
-    N = cfg["n"]; L = N // world
+    N = cfg["n"]
+    ln, ls, la, active = slab.configuration_1d(N, world, rank)
     rng = np.random.Generator(np.random.MT19937(9))
     g = rng.uniform(-1, 1, N) + 1j * rng.uniform(-1, 1, N)
     plan = slab.FFT1D()
-    rc = plan.init(N, L, rank * L, S.Z2Z, None, device_ops=NumpyOps())
-    out = {"rank": rank, "init": rc}
+    rc = plan.init(N, ln, ls, S.Z2Z, None, device_ops=NumpyOps())
+    out = {"rank": rank, "init": rc, "local": [ln, ls, la, active]}
     if rc == 0:
         assert plan.plan() == 0
-        a = torch.zeros(L, dtype=torch.complex128); b = torch.zeros_like(a)
+        out["path"] = plan.path
+        assert plan.alloc_size() == la
+        a = torch.zeros(max(la, 1), dtype=torch.complex128); b = torch.full_like(a, 7.0)
         assert plan.set_buffers(a, b) == 0
-        _, d, _ = plan.get_buffers(); d[:] = torch.from_numpy(g[rank * L:(rank + 1) * L])
+        _, d, _ = plan.get_buffers(); d[:ln] = torch.from_numpy(g[ls:ls + ln])
         assert plan.execute(S.FORWARD) == 0
         _, d2, _ = plan.get_buffers()
-        out["swapped"] = d2.data_ptr() != d.data_ptr()
-        ref = np.fft.fft(g)[rank * L:(rank + 1) * L]
-        out["fwd_err"] = float(np.abs(d2.numpy() - ref).max() / np.abs(ref).max())
+        out["swapped"] = d2.data_ptr() != d.data_ptr() or la == 0
+        ref = np.fft.fft(g)[ls:ls + ln]
+        out["fwd_err"] = float(np.abs(d2[:ln].numpy() - ref).max() / np.abs(np.fft.fft(g)).max()) if ln else 0.0
         assert plan.execute(S.BACKWARD) == 0 and plan.normalize() == 0
         _, d3, _ = plan.get_buffers()
-        out["rt_err"] = float(np.abs(d3.numpy() - g[rank * L:(rank + 1) * L]).max())
+        out["rt_err"] = float(np.abs(d3[:ln].numpy() - g[ls:ls + ln]).max()) if ln else 0.0
+        plan.release()
     dist.destroy_process_group()
     json.dump(out, open(sys.argv[2], "w"))
     sys.exit(0)
@@ -215,10 +239,35 @@ def test_slab_fft1d_four_step_on_gloo_ranks(tmp_path, world, n):
         assert o["rt_err"] < 1e-12, o
 
 
-def test_slab_fft1d_needs_p_squared(tmp_path):
-    import shafft_b200 as S
-    res = _run(tmp_path, 2, {"fft1d": True, "n": 6})   # 6 % 4 != 0
-    assert all(o["init"] == S.ERR_NOT_IMPL for o in res)
+@pytest.mark.parametrize("world,n,path,active", [
+    (2, 6, "cooley_tukey", 1),      # Bluestein on 2 leaves rank 1 empty: one active rank
+    (3, 1001, "bluestein", 2),      # M = 1004 over 2 active ranks, the second holding nothing
+    (6, 1001, "bluestein", 3),      # ranks 0-2 active (669 + 332 + 0 points), 3-5 inactive
+    (3, 1000, "cooley_tukey", 2),   # re-chosen for the 2 active ranks: 4 divides 1000
+    (4, 97 * 13, "bluestein", 2)])
+def test_slab_fft1d_bluestein_and_inactive_ranks(tmp_path, world, n, path, active):
+    """Lengths that P^2 does not divide: the reference's layout query (empty
+    blocks -> inactive ranks, path chosen again for the active ones) and
+    path B, Bluestein over the distributed four-step."""
+    res = _run(tmp_path, world, {"fft1d": True, "n": n})
+    assert sum(o["local"][0] for o in res) == n
+    for o in res:
+        assert o["init"] == 0 and o["local"][3] == active
+        assert o["local"] == list(slab.configuration_1d(n, world, o["rank"]))
+        if o["rank"] < active:
+            assert o["path"] == path
+        assert o["fwd_err"] < 1e-12, o
+        assert o["rt_err"] < 1e-12, o
+
+
+def test_select_path_and_layout_rules():
+    assert slab.select_path_1d(1 << 20, 2) == ("cooley_tukey", 1 << 20, 1 << 19)
+    assert slab.select_path_1d(1000003, 4) == ("bluestein", 2000016, 500004)  # ceil(1999/16)*16
+    assert slab.select_path_1d(7, 1) == ("cooley_tukey", 7, 7)
+    # blocks of the re-chosen size, start clamped to N on empty active ranks
+    assert [slab.configuration_1d(1001, 6, r) for r in range(6)] == [
+        (669, 0, 669, 3), (332, 669, 669, 3), (0, 1001, 669, 3), (0, 0, 0, 3), (0, 0, 0, 3), (0, 0, 0, 3)]
+    assert slab.configuration_1d(5, 1, 0) == (5, 0, 5, 1)
 
 
 def test_configuration_nd_decomposition_search():
