@@ -249,7 +249,7 @@ def test_bluestein_chirp_kernels(prec, n, m, n0, m0, count):
     mm = m0 + i
     j = np.where(mm < n, mm, np.where((mm > m - n) & (mm < m), m - mm, -1))
     v_ref = np.where(j >= 0, _chirp_ref(np.maximum(j, 0), n, 1), 0)
-    t = 2e-7 if prec == S.C2C else 1e-15
+    t = 2e-7 if prec == S.C2C else 4e-15  # a few ulp: sincospi on the GPU, exp in numpy
     assert np.abs(b.cpu().numpy() - b_ref).max() <= t
     assert np.abs(v.cpu().numpy() - v_ref).max() <= t
     dt = np.complex128 if prec == S.Z2Z else np.complex64
