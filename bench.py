@@ -182,6 +182,18 @@ def cpu_sample(threads=None, dims=(256, 256, 256)):
     return step_bytes(dims) / t / 1e9, t, threads, err
 
 
+def cpu_model():
+    """Host CPU model name (Linux /proc/cpuinfo), recorded beside the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -207,7 +219,7 @@ def reference_arm(args):
         "config": {"workload": "FFTND complex C2C fwd+bwd with normalize, bounded CPU sample",
                    "dims": list(dims), "threads": threads},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "roundtrip_rel_l2": err,
     }
@@ -366,7 +378,8 @@ def ours(args):
         v, t, thr, err = cpu_sample()
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
                "sample": f"256x256x256 complex64 fwd+normalize+bwd+normalize, FP64 oracle "
-                         f"(oracle/oracle_fft.c), {thr} threads, {t:.2f} s"}
+                         f"(oracle/oracle_fft.c), {thr} threads, {t:.2f} s",
+               "cpu_model": cpu_model()}
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
