@@ -307,6 +307,23 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
 #pragma unroll
         for (int r = 0; r < RL; ++r) x[r][e] = y[r];
       }
+      // four-step twiddle w_N^{k t} over this thread's outputs k = kbase +
+      // r*KSTRIDE: a running product twc *= w_N^{KSTRIDE t}, taken afresh
+      // from the two-level table every kTwAnchor outputs, so each element
+      // needs (2 + 2*RL/kTwAnchor)/RL table reads instead of 2 (the reads
+      // are scattered when t differs per lane) and carries at most
+      // kTwAnchor - 1 extra roundings.
+      constexpr int kTwAnchor = 4;
+      C twc[VW], tws[VW];
+      int64_t tcol[VW];
+      if (g.tw_mode == TW_POST) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+          tcol[e] = (g.tw_dim == 0) ? (w0 + c * VW + e) : tconst;
+          const int64_t ms = (int64_t)KSTRIDE * tcol[e];
+          tws[e] = cmul(ld_tw(tb.tw_hi + (ms >> g.tw_shift)), ld_tw(tb.tw_lo + (ms & g.tw_mask)));
+        }
+      }
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
         const int k = kbase + r * KSTRIDE;
@@ -315,9 +332,13 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
         for (int e = 0; e < VW; ++e) {
           C y = x[r][e];
           if (g.tw_mode == TW_POST) {
-            const int64_t t = (g.tw_dim == 0) ? (w0 + c * VW + e) : tconst;
-            const int64_t m = (int64_t)k * t;
-            y = cmul(y, cmul(ld_tw(tb.tw_hi + (m >> g.tw_shift)), ld_tw(tb.tw_lo + (m & g.tw_mask))));
+            if (r % kTwAnchor == 0) {
+              const int64_t m = (int64_t)k * tcol[e];
+              twc[e] = cmul(ld_tw(tb.tw_hi + (m >> g.tw_shift)), ld_tw(tb.tw_lo + (m & g.tw_mask)));
+            } else {
+              twc[e] = cmul(twc[e], tws[e]);
+            }
+            y = cmul(y, twc[e]);
           }
           if (g.scale != 1.0) y = cscale(y, scale);
           if (g.conj_out) y.y = -y.y;
