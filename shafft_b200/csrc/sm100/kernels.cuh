@@ -295,57 +295,101 @@ __global__ void k_scale_copy(const typename Cx<T>::type* src, typename Cx<T>::ty
   }
 }
 
+// The Bluestein element-wise steps run on a 2-D grid: blockIdx.y walks the
+// batch rows b = o*I + i (one division per row), blockIdx.x/threadIdx.x the
+// points of a row in block tiles of kEwUnroll*blockDim points, each thread
+// loading its kEwUnroll points before it computes (independent loads in
+// flight; the arrays are L2-resident at the lengths Bluestein pads to).
+constexpr int kEwUnroll = 4;
+
 // Bluestein modulate: dst[b*M + m] = (m < L) ? conj?(x(o, m, i)) * chirp[m] : 0
 // with b = o*I + i and x(o, m, i) = src[(o*L + m)*I + i].
 template <typename T>
 __global__ void k_bs_modulate(const typename Cx<T>::type* src, typename Cx<T>::type* dst, int64_t L,
-                              int64_t M, int64_t I, int64_t total, const typename Cx<T>::type* chirp,
+                              int64_t M, int64_t I, int64_t rows, const typename Cx<T>::type* chirp,
                               int conj) {
   using C = typename Cx<T>::type;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = idx / M, m = idx - b * M;
-    C r = C{0, 0};
-    if (m < L) {
-      const int64_t o = b / I, i = b - o * I;
-      C x = src[(o * L + m) * I + i];
-      if (conj) x.y = -x.y;
-      r = cmul(x, chirp[m]);
+  const int64_t tile = (int64_t)blockDim.x * kEwUnroll;
+  for (int64_t b = blockIdx.y; b < rows; b += gridDim.y) {
+    const int64_t o = b / I, i = b - o * I;
+    const C* srow = src + o * L * I + i;
+    C* drow = dst + b * M;
+    for (int64_t base = blockIdx.x * tile + threadIdx.x; base < M; base += gridDim.x * tile) {
+      C x[kEwUnroll], w[kEwUnroll];
+#pragma unroll
+      for (int u = 0; u < kEwUnroll; ++u) {
+        const int64_t m = base + (int64_t)u * blockDim.x;
+        x[u] = m < L ? srow[m * I] : C{0, 0};
+        w[u] = m < L ? chirp[m] : C{0, 0};
+      }
+#pragma unroll
+      for (int u = 0; u < kEwUnroll; ++u) {
+        const int64_t m = base + (int64_t)u * blockDim.x;
+        if (conj) x[u].y = -x[u].y;
+        if (m < M) drow[m] = cmul(x[u], w[u]);
+      }
     }
-    dst[idx] = r;
   }
 }
 
-// s[idx] = conj(s[idx] * H[idx % M])   (H carries the 1/M of the inverse)
+// s[b*M + m] = conj(s[b*M + m] * H[m])   (H carries the 1/M of the inverse)
 template <typename T>
 __global__ void k_bs_mulh(typename Cx<T>::type* s, const typename Cx<T>::type* H, int64_t M,
-                          int64_t total) {
+                          int64_t rows) {
   using C = typename Cx<T>::type;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    C y = cmul(s[idx], H[idx % M]);
-    y.y = -y.y;
-    s[idx] = y;
+  const int64_t tile = (int64_t)blockDim.x * kEwUnroll;
+  for (int64_t b = blockIdx.y; b < rows; b += gridDim.y) {
+    C* row = s + b * M;
+    for (int64_t base = blockIdx.x * tile + threadIdx.x; base < M; base += gridDim.x * tile) {
+      C x[kEwUnroll], h[kEwUnroll];
+#pragma unroll
+      for (int u = 0; u < kEwUnroll; ++u) {
+        const int64_t m = base + (int64_t)u * blockDim.x;
+        x[u] = m < M ? row[m] : C{0, 0};
+        h[u] = m < M ? H[m] : C{0, 0};
+      }
+#pragma unroll
+      for (int u = 0; u < kEwUnroll; ++u) {
+        const int64_t m = base + (int64_t)u * blockDim.x;
+        C y = cmul(x[u], h[u]);
+        y.y = -y.y;
+        if (m < M) row[m] = y;
+      }
+    }
   }
 }
 
 // Bluestein demodulate: dst(o, k, i) = conj?(chirp[k] * conj(s[b*M + k])) * scale
 template <typename T>
 __global__ void k_bs_demod(const typename Cx<T>::type* s, typename Cx<T>::type* dst, int64_t L,
-                           int64_t M, int64_t I, int64_t total, const typename Cx<T>::type* chirp,
+                           int64_t M, int64_t I, int64_t rows, const typename Cx<T>::type* chirp,
                            int conj, T scale) {
   using C = typename Cx<T>::type;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = idx / L, k = idx - b * L;
+  const int64_t tile = (int64_t)blockDim.x * kEwUnroll;
+  for (int64_t b = blockIdx.y; b < rows; b += gridDim.y) {
     const int64_t o = b / I, i = b - o * I;
-    C v = s[b * M + k];
-    v.y = -v.y;
-    C r = cmul(chirp[k], v);
-    r.x *= scale;
-    r.y *= scale;
-    if (conj) r.y = -r.y;
-    dst[(o * L + k) * I + i] = r;
+    const C* srow = s + b * M;
+    C* drow = dst + o * L * I + i;
+    for (int64_t base = blockIdx.x * tile + threadIdx.x; base < L; base += gridDim.x * tile) {
+      C v[kEwUnroll], w[kEwUnroll];
+#pragma unroll
+      for (int u = 0; u < kEwUnroll; ++u) {
+        const int64_t k = base + (int64_t)u * blockDim.x;
+        v[u] = k < L ? srow[k] : C{0, 0};
+        w[u] = k < L ? chirp[k] : C{0, 0};
+      }
+#pragma unroll
+      for (int u = 0; u < kEwUnroll; ++u) {
+        const int64_t k = base + (int64_t)u * blockDim.x;
+        C a = v[u];
+        a.y = -a.y;
+        C r = cmul(w[u], a);
+        r.x *= scale;
+        r.y *= scale;
+        if (conj) r.y = -r.y;
+        if (k < L) drow[k * I] = r;
+      }
+    }
   }
 }
 

@@ -15,6 +15,17 @@
 
 namespace shafft_sm100 {
 
+// 2-D grid of 256-thread blocks over `rows` rows of `len` points (block
+// tiles of kEwUnroll*256 points): at most one wave of 8 blocks per SM, rows
+// in y (<= 65535).
+static inline dim3 row_grid(int64_t rows, int64_t len) {
+  const int64_t cap = 148 * 8;
+  const int64_t per = 256 * kEwUnroll;
+  const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((len + per - 1) / per, cap));
+  const int64_t gy = std::max<int64_t>(1, std::min<int64_t>({rows, std::max<int64_t>(1, cap / gx), 65535}));
+  return dim3((unsigned)gx, (unsigned)gy, 1);
+}
+
 static inline unsigned ew_grid(int64_t n) {
   int64_t g = (n + 255) / 256;
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
@@ -369,20 +380,26 @@ cudaError_t Launch<T>::scale_copy(const C* src, C* dst, int64_t n, T factor, int
 template <typename T>
 cudaError_t Launch<T>::bs_modulate(const C* src, C* dst, int64_t L, int64_t M, int64_t I,
                                    int64_t total, const C* chirp, int conj, cudaStream_t s) {
-  k_bs_modulate<T><<<ew_grid(total), 256, 0, s>>>(src, dst, L, M, I, total, chirp, conj);
+  const int64_t rows = M > 0 ? total / M : 0;
+  if (rows == 0) return cudaSuccess;
+  k_bs_modulate<T><<<row_grid(rows, M), 256, 0, s>>>(src, dst, L, M, I, rows, chirp, conj);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t Launch<T>::bs_mulh(C* d, const C* H, int64_t M, int64_t total, cudaStream_t s) {
-  k_bs_mulh<T><<<ew_grid(total), 256, 0, s>>>(d, H, M, total);
+  const int64_t rows = M > 0 ? total / M : 0;
+  if (rows == 0) return cudaSuccess;
+  k_bs_mulh<T><<<row_grid(rows, M), 256, 0, s>>>(d, H, M, rows);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t Launch<T>::bs_demod(const C* src, C* dst, int64_t L, int64_t M, int64_t I, int64_t total,
                                 const C* chirp, int conj, T scale, cudaStream_t s) {
-  k_bs_demod<T><<<ew_grid(total), 256, 0, s>>>(src, dst, L, M, I, total, chirp, conj, scale);
+  const int64_t rows = L > 0 ? total / L : 0;
+  if (rows == 0) return cudaSuccess;
+  k_bs_demod<T><<<row_grid(rows, L), 256, 0, s>>>(src, dst, L, M, I, rows, chirp, conj, scale);
   return cudaGetLastError();
 }
 
