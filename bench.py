@@ -588,7 +588,10 @@ def suite_batched(args):
         for i, s in enumerate(shapes):
             plans[s].execute(cp[i], dp[i], 0, 1.0, stream.cuda_stream)
     scr.copy_(src)
-    plain()
+    # two untimed passes: a plan replays a launch sequence it has seen twice
+    # (graph replay of executes), so the timed passes run at steady state
+    for _ in range(2):
+        plain()
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(2):

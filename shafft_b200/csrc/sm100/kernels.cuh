@@ -236,25 +236,41 @@ __device__ __forceinline__ void generic_tile(const PassGeom& g, const typename C
     }
   }
   // phase 3: digit-reversed read, fused twiddle/scale/conj, store
-  {
-    const int total = L << logW;
-    const T scale = (T)g.scale;
+  const int total = L << logW;
+  const T scale = (T)g.scale;
+  if (g.out_row) {
     for (int b = threadIdx.x; b < total; b += kThreads) {
-      int w, p, k;
-      if (g.out_row) {
-        k = b % L;
-        w = b / L;
-        p = tb.k2p[k];
-      } else {
-        w = b & (W - 1);
-        p = b >> logW;
-        k = tb.p2k[p];
-      }
+      const int k = b % L, w = b / L;
       if (w >= wcount) continue;
-      C x = sm[p * pitch + w];
+      C x = sm[tb.k2p[k] * pitch + w];
       if (g.tw_mode == TW_POST) {
         const int64_t t = (g.tw_dim == 0) ? (w0 + w) : tconst;
         x = cmul(x, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * t));
+      }
+      if (g.scale != 1.0) x = cscale(x, scale);
+      if (g.conj_out) x.y = -x.y;
+      out[bout + (int64_t)w * g.sout[0] + (int64_t)k * g.sk_out] = x;
+    }
+  } else {
+    // column output walked in natural k order: a thread keeps its column
+    // w = tid mod W (W divides kThreads) and visits k = k0, k0 + KS, ...
+    // (KS = kThreads / W), so the four-step twiddle w_N^{k t} is a running
+    // product by w_N^{KS t}, taken afresh from the table every 4 outputs
+    // (the table reads are scattered across the lanes)
+    const int KS = kThreads >> logW;
+    const int w = threadIdx.x & (W - 1);
+    const bool tw = g.tw_mode == TW_POST && w < wcount;
+    const int64_t t = (g.tw_dim == 0) ? (w0 + w) : tconst;
+    C tstep = C{1, 0}, tcur = C{1, 0};
+    if (tw && KS < L) tstep = tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)KS * t);
+    int i = 0;
+    for (int b = threadIdx.x; b < total; b += kThreads, ++i) {
+      if (w >= wcount) continue;
+      const int k = b >> logW;
+      C x = sm[tb.k2p[k] * pitch + w];
+      if (tw) {
+        tcur = (i % 4 == 0) ? tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * t) : cmul(tcur, tstep);
+        x = cmul(x, tcur);
       }
       if (g.scale != 1.0) x = cscale(x, scale);
       if (g.conj_out) x.y = -x.y;

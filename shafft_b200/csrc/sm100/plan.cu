@@ -919,6 +919,7 @@ struct shafft_sm100_plan_s {
   cudaStream_t capture_stream = nullptr;
   bool graphs_off = false;
   uint64_t graph_clock = 0;
+  int graph_evictions = 0;  // replay turns itself off for callers that cycle through many buffers
 };
 
 namespace {
@@ -1541,6 +1542,15 @@ int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direc
   for (auto& g : plan->graphs)
     if (g.src == src && g.dst == dst && g.dir == direction && g.scale == scale) e = &g;
   if (!e) {
+    if (plan->graphs.size() >= 8 && ++plan->graph_evictions > 8) {
+      // the caller cycles through more (src, dst) pairs than the plan keeps:
+      // captures would rarely be replayed, so run eagerly from now on
+      for (auto& g : plan->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+      plan->graphs.clear();
+      plan->graphs_off = true;
+      return eager(s);
+    }
     if (plan->graphs.size() >= 8) {  // evict the least recently used
       auto lru = std::min_element(plan->graphs.begin(), plan->graphs.end(),
                                   [](const Plan::GraphEntry& x, const Plan::GraphEntry& y) { return x.last < y.last; });

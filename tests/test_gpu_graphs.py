@@ -35,3 +35,26 @@ def test_replayed_executes_match_eager(dims, prec, flags):
     ref = o.fftn(x.astype(np.complex128), precise=bool(prec)).ravel()
     tol = (1e-6 if prec == 0 else 1e-14) * max(1.0, np.log2(n))
     assert o.rel_l2(first[(0, 1.0, True)], ref) <= tol
+
+
+def test_many_buffer_pairs_fall_back_to_eager():
+    """A plan executed on more (src, dst) pairs than it keeps graphs for
+    evicts, then turns replay off; every result stays identical to the
+    first eager execute of the same input."""
+    dims = (64, 48, 40)
+    plan = _sm100.Plan(dims, 0, 0)
+    x = o.uniform_input(dims, seed=9, dtype=np.complex64)
+    n = x.size
+    pairs = [(S.DeviceBuffer(n, 0), S.DeviceBuffer(n, 0)) for _ in range(20)]
+    want = None
+    for rep in range(3):
+        for src, dst in pairs:
+            src.upload(x)
+            plan.execute(src.ptr, dst.ptr, 0, 1.0, 0)
+            plan.status()
+            y = dst.download()
+            if want is None:
+                want = y
+            assert np.array_equal(y, want), rep
+    ref = o.fftn(x.astype(np.complex128)).ravel()
+    assert o.rel_l2(want, ref) <= 1e-6 * np.log2(n)
