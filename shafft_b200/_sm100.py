@@ -151,6 +151,11 @@ class Plan:
     def passes(self) -> int:
         return self._lib.shafft_sm100_plan_passes(self.handle)
 
+    @property
+    def device_bytes(self) -> int:
+        """Device memory the plan holds (tables and scratch)."""
+        return int(self._lib.shafft_sm100_plan_device_bytes(self.handle))
+
     def destroy(self):
         if self.handle:
             self._lib.shafft_sm100_plan_destroy(self.handle)

@@ -1055,7 +1055,20 @@ struct Launcher {
   }
 
   // Build every table of the plan on the device.
+  // Every table of the plan, generated on the plan's stream with one
+  // synchronisation at the end.  The digit tables are copied from pageable
+  // host memory first, while the stream is still empty (such a copy waits
+  // for the stream's earlier work before it starts; under a server's load
+  // that wait is behind other transforms' kernels).
   static int build_tables(shafft_sm100_plan_s* p) {
+    for (const LTable& lt : p->ltabs) {
+      std::vector<uint16_t> p2k, k2p;
+      digit_tables(lt.L, p2k, k2p);
+      CUDA_TRY(cudaMemcpyAsync(p->d_tables + lt.off_p2k, p2k.data(), 2 * lt.L,
+                               cudaMemcpyHostToDevice, p->stream));
+      CUDA_TRY(cudaMemcpyAsync(p->d_tables + lt.off_k2p, k2p.data(), 2 * lt.L,
+                               cudaMemcpyHostToDevice, p->stream));
+    }
     for (const LTable& lt : p->ltabs) {
       if (lt.tc_bytes) {
         const int rc = tc_gen_table(p->d_tables + lt.off_tcB, lt.L, p->stream);
@@ -1065,13 +1078,6 @@ struct Launcher {
                                     p->stream),
                      "twiddle generation");
       if (rc) return rc;
-      std::vector<uint16_t> p2k, k2p;
-      digit_tables(lt.L, p2k, k2p);
-      CUDA_TRY(cudaMemcpyAsync(p->d_tables + lt.off_p2k, p2k.data(), 2 * lt.L,
-                               cudaMemcpyHostToDevice, p->stream));
-      CUDA_TRY(cudaMemcpyAsync(p->d_tables + lt.off_k2p, k2p.data(), 2 * lt.L,
-                               cudaMemcpyHostToDevice, p->stream));
-      CUDA_TRY(cudaStreamSynchronize(p->stream));
     }
     for (const NTable& nt : p->ntabs) {
       int rc = check(K::gen_twiddle(reinterpret_cast<C*>(p->d_tables + nt.off_hi), nt.nhi, nt.nlo,

@@ -2,7 +2,14 @@
 //
 // Clients submit C2C transforms (shape, precision, direction, scale, host
 // input and output buffers) from any thread.  A dispatcher thread admits
-// requests in arrival order as soon as their device memory fits the budget:
+// requests in arrival order as soon as their device memory fits the budget
+// and a plan instance of their shape is free; a request whose shape has no
+// free instance asks a builder thread for one and lets the requests behind it
+// (up to kScanWindow) go first, so plan creation (device allocations, table
+// kernels, a synchronisation: tens of ms for large shapes) overlaps the
+// transforms instead of stalling the queue.  Memory admission stays in
+// arrival order: a request that does not fit the budget holds back the ones
+// behind it.
 //   * device input/output buffers come from a stream-ordered memory pool
 //     (cudaMallocAsync / cudaFreeAsync), so freeing is ordered after the work;
 //   * plans are kept resident per shape (several instances per shape when
@@ -105,6 +112,17 @@ struct shafft_sm100_server_s {
   // plan-instance churn: creations (and their wall time) and evictions
   uint64_t plans_created = 0, plans_evicted = 0;
   double create_ms_total = 0, create_ms_max = 0;
+  // background plan creation: shapes waiting for an instance (one build in
+  // flight per shape)
+  struct BuildJob {
+    std::string key;
+    std::vector<int64_t> dims;
+    int precision;
+  };
+  std::deque<BuildJob> build_q;
+  std::map<std::string, int> building;
+  std::condition_variable cv_build;
+  std::thread builder;
 };
 
 namespace {
@@ -115,57 +133,98 @@ std::string plan_key(const Request& r) {
   return k;
 }
 
-// caller holds s->mu (locked in `lk`); returns a free plan instance for r,
-// creating one when every instance of the shape is busy.  Creation (device
-// allocations, table kernels, a synchronisation) runs with the lock released
-// so that completions keep flowing meanwhile.
-PlanInst* acquire_plan(shafft_sm100_server_s* s, std::unique_lock<std::mutex>& lk, const Request& r,
-                       int* rc) {
+constexpr size_t kScanWindow = 64;  // queued requests the dispatcher looks past a plan-blocked one
+
+// caller holds s->mu: a free instance of r's shape (marked busy), or null
+// after asking the builder for one (unless a build of that shape runs)
+PlanInst* free_instance(shafft_sm100_server_s* s, const Request& r) {
   const std::string key = plan_key(r);
-  for (auto& p : s->plans[key])
-    if (!p->busy) {
-      p->busy = true;
-      p->last_used = Clock::now();
-      return p.get();
+  auto it = s->plans.find(key);
+  if (it != s->plans.end())
+    for (auto& p : it->second)
+      if (!p->busy) {
+        p->busy = true;
+        p->last_used = Clock::now();
+        return p.get();
+      }
+  if (!s->building.count(key)) {
+    s->building[key] = 1;
+    s->build_q.push_back(shafft_sm100_server_s::BuildJob{key, r.dims, r.precision});
+    s->cv_build.notify_one();
+  }
+  return nullptr;
+}
+
+// Creates the plan instances the dispatcher asks for, with the lock released
+// while a plan is built so that admissions and completions keep flowing.  A
+// shape whose plan cannot be created fails its queued requests.
+void builder_loop(shafft_sm100_server_s* s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop) {
+    if (s->build_q.empty()) {
+      s->cv_build.wait_for(lk, std::chrono::milliseconds(20));
+      continue;
     }
-  lk.unlock();
-  shafft_sm100_plan pl = nullptr;
-  const auto t0 = Clock::now();
-  *rc = shafft_sm100_plan_create_nd(&pl, (int)r.dims.size(), r.dims.data(), r.precision);
-  const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
-  lk.lock();
-  s->plans_created++;
-  s->create_ms_total += ms;
-  s->create_ms_max = std::max(s->create_ms_max, ms);
-  if (*rc) return nullptr;
-  auto inst = std::make_unique<PlanInst>();
-  inst->plan = pl;
-  inst->bytes = shafft_sm100_plan_device_bytes(pl);
-  inst->busy = true;
-  inst->last_used = Clock::now();
-  s->plan_bytes += inst->bytes;
-  s->used += inst->bytes;
-  auto& vec = s->plans[key];
-  vec.push_back(std::move(inst));
-  return vec.back().get();
+    const shafft_sm100_server_s::BuildJob job = s->build_q.front();
+    s->build_q.pop_front();
+    lk.unlock();
+    shafft_sm100_plan pl = nullptr;
+    const auto t0 = Clock::now();
+    const int rc = shafft_sm100_plan_create_nd(&pl, (int)job.dims.size(), job.dims.data(), job.precision);
+    const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    lk.lock();
+    s->plans_created++;
+    s->create_ms_total += ms;
+    s->create_ms_max = std::max(s->create_ms_max, ms);
+    s->building.erase(job.key);
+    if (rc) {
+      for (auto it = s->queue.begin(); it != s->queue.end();) {
+        if (plan_key(**it) == job.key) {
+          (*it)->status = rc;
+          (*it)->done = true;
+          (*it)->t_done = Clock::now();
+          s->failed++;
+          it = s->queue.erase(it);
+        } else {
+          ++it;
+        }
+      }
+      s->cv_done.notify_all();
+    } else {
+      auto inst = std::make_unique<PlanInst>();
+      inst->plan = pl;
+      inst->bytes = shafft_sm100_plan_device_bytes(pl);
+      inst->last_used = Clock::now();
+      s->plan_bytes += inst->bytes;
+      s->used += inst->bytes;
+      s->plans[job.key].push_back(std::move(inst));
+    }
+    s->cv_queue.notify_all();
+  }
 }
 
 // caller holds s->mu: unlink idle plan instances, oldest first, until the
-// resident plans leave room for `need` bytes.  Buffers of requests in flight
+// resident plans leave room for `need` bytes, keeping the instances of the
+// shape `keep_key` (the request the room is made for would otherwise lose the
+// plan it waits for and ask for it again).  Buffers of requests in flight
 // are not counted: they come back as those requests complete, so waiting for
 // them is cheaper than destroying and later re-creating plans.  The unlinked plans are returned in `dead` and
 // destroyed by the caller after it drops the lock (cudaFree synchronises the
 // device, which must not happen while completions wait for the lock).
-void evict_idle(shafft_sm100_server_s* s, size_t need, std::vector<shafft_sm100_plan>& dead) {
+void evict_idle(shafft_sm100_server_s* s, size_t need, const std::string& keep_key,
+                std::vector<shafft_sm100_plan>& dead) {
   while (s->plan_bytes + need > s->budget) {
     PlanInst* victim = nullptr;
     std::string vkey;
-    for (auto& kv : s->plans)
+    for (auto& kv : s->plans) {
+      if (kv.first == keep_key) continue;  // the waiting request's own shape
       for (auto& p : kv.second)
         if (!p->busy && (!victim || p->last_used < victim->last_used)) {
           victim = p.get();
           vkey = kv.first;
         }
+    }
     if (!victim) return;
     auto& vec = s->plans[vkey];
     for (size_t i = 0; i < vec.size(); ++i)
@@ -189,43 +248,49 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
       s->cv_queue.wait_for(lk, std::chrono::milliseconds(20));
       continue;
     }
-    std::shared_ptr<Request> r = s->queue.front();
-    const size_t need = 2 * r->bytes;
-    if (s->plan_bytes + need > s->budget) {
-      std::vector<shafft_sm100_plan> dead;
-      evict_idle(s, need, dead);
-      if (!dead.empty()) {
-        lk.unlock();
-        for (auto pl : dead) shafft_sm100_plan_destroy(pl);
-        lk.lock();
+    {
+      std::shared_ptr<Request> head = s->queue.front();
+      const size_t hneed = 2 * head->bytes;
+      if (s->plan_bytes + hneed > s->budget) {
+        std::vector<shafft_sm100_plan> dead;
+        evict_idle(s, hneed, plan_key(*head), dead);
+        if (!dead.empty()) {
+          lk.unlock();
+          for (auto pl : dead) shafft_sm100_plan_destroy(pl);
+          lk.lock();
+          continue;  // the queue may have changed meanwhile
+        }
       }
-    }
-    if (s->used + need > s->budget) {
-      if (s->inflight.empty()) {
+      if (s->used + hneed > s->budget && s->inflight.empty() && s->building.empty()) {
         // can never fit: fail it instead of blocking the queue
         s->queue.pop_front();
-        r->status = sfail(SHAFFT_SM100_EALLOC, "request needs %zu bytes, budget %zu", need, s->budget);
-        r->done = true;
-        r->t_done = Clock::now();
+        head->status = sfail(SHAFFT_SM100_EALLOC, "request needs %zu bytes, budget %zu", hneed, s->budget);
+        head->done = true;
+        head->t_done = Clock::now();
         s->failed++;
         s->cv_done.notify_all();
         continue;
       }
-      // wait for completions to free budget (FIFO admission)
+    }
+    // the first request, in arrival order, that fits the budget and has a
+    // free plan instance; a request that does not fit stops the scan
+    std::shared_ptr<Request> r;
+    PlanInst* inst = nullptr;
+    size_t pos = 0;
+    for (auto it = s->queue.begin(); it != s->queue.end() && pos < kScanWindow; ++it, ++pos) {
+      if (s->used + 2 * (*it)->bytes > s->budget) break;
+      inst = free_instance(s, **it);
+      if (inst) {
+        r = *it;
+        s->queue.erase(it);
+        break;
+      }
+    }
+    if (!r) {
       s->cv_queue.wait_for(lk, std::chrono::microseconds(200));
       continue;
     }
-    s->queue.pop_front();
-    int rc = 0;
-    PlanInst* inst = acquire_plan(s, lk, *r, &rc);
-    if (!inst) {
-      r->status = rc;
-      r->done = true;
-      r->t_done = Clock::now();
-      s->failed++;
-      s->cv_done.notify_all();
-      continue;
-    }
+    const size_t need = 2 * r->bytes;
     s->used += need;
     // least recently used stream
     int si = 0;
@@ -340,6 +405,7 @@ int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, in
   }
   s->dispatcher = std::thread(dispatcher_loop, s);
   s->completer = std::thread(completer_loop, s);
+  s->builder = std::thread(builder_loop, s);
   *out = s;
   return 0;
 }
@@ -422,9 +488,11 @@ int shafft_sm100_server_destroy(shafft_sm100_server s) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
     s->cv_queue.notify_all();
+    s->cv_build.notify_all();
   }
   s->dispatcher.join();
   s->completer.join();
+  s->builder.join();
   for (auto st : s->streams) {
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);

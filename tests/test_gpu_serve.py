@@ -65,3 +65,65 @@ def test_budget_too_small_fails_cleanly():
     with pytest.raises(_sm100.Sm100Error):
         srv.wait(rid)
     srv.destroy()
+
+
+def _check_result(x, b, prec, direction):
+    ref = o.fftn(x.astype(np.complex128), sign=-1 if direction == 0 else 1, precise=bool(prec))
+    tol = (1e-6 if prec == 0 else 1e-14) * max(1.0, math.log2(x.size))
+    assert o.rel_l2(b.numpy(), ref) <= tol
+
+
+@pytest.mark.timeout(300)
+def test_plan_builds_run_beside_other_requests():
+    """A request whose shape needs a new plan (built by the server's builder
+    thread) does not hold back the requests queued behind it; every result
+    is correct."""
+    srv = _sm100.Server(budget_bytes=8 << 30, streams=4)
+    small = (64, 64, 32)
+    xs = o.uniform_input(small, seed=2, dtype=np.complex64)
+    a0, b0 = pinned(xs), pinned(np.zeros_like(xs))
+    srv.wait(srv.submit(small, 0, 0, 1.0, a0.data_ptr(), b0.data_ptr()))  # plan resident
+    big = (256, 256, 128)
+    xb = o.uniform_input(big, seed=3, dtype=np.complex64)
+    ab, bb = pinned(xb), pinned(np.zeros_like(xb))
+    rid_big = srv.submit(big, 0, 0, 1.0, ab.data_ptr(), bb.data_ptr())
+    reqs = []
+    for i in range(24):
+        x = o.uniform_input(small, seed=100 + i, dtype=np.complex64)
+        a, b = pinned(x), pinned(np.zeros_like(x))
+        reqs.append((srv.submit(small, 0, i % 2, 1.0, a.data_ptr(), b.data_ptr()), x, a, b, i % 2))
+    for rid, x, a, b, d in reqs:
+        srv.wait(rid)
+        _check_result(x, b, 0, d)
+    srv.wait(rid_big)
+    _check_result(xb, bb, 0, 0)
+    st = srv.stats()
+    assert st["failed"] == 0 and st["completed"] == 26
+    assert st["plans_created"] >= 2
+    srv.destroy()
+
+
+@pytest.mark.timeout(300)
+def test_tight_budget_alternating_shapes_evicts_and_completes():
+    """A budget that holds one Bluestein plan (its scratch and kernel
+    spectrum are several times the request's buffers) and its buffers at a
+    time: alternating prime lengths must evict the other shape's idle plan
+    (never the waiting request's own) and every request completes
+    correctly."""
+    A, B = (1000003,), (999983,)
+    need = [2 * 8 * math.prod(s) + _sm100.Plan(s, 0).device_bytes for s in (A, B)]
+    budget = max(need) + (1 << 20)
+    assert budget < sum(need)
+    srv = _sm100.Server(budget_bytes=budget, streams=2)
+    reqs = []
+    for i, s in enumerate([A, B, A, B, A, B]):
+        x = o.uniform_input(s, seed=200 + i, dtype=np.complex64)
+        a, b = pinned(x), pinned(np.zeros_like(x))
+        reqs.append((srv.submit(s, 0, 0, 1.0, a.data_ptr(), b.data_ptr()), x, a, b))
+    for rid, x, a, b in reqs:
+        srv.wait(rid)
+        _check_result(x, b, 0, 0)
+    st = srv.stats()
+    assert st["failed"] == 0 and st["completed"] == 6
+    assert st["plans_evicted"] >= 1
+    srv.destroy()
