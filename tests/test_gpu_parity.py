@@ -1,7 +1,7 @@
 """GPU parity of the sm_100a path against the CPU oracle and the golden
 vectors, through the SHAFFT C ABI (libshafft.so -> libshafft_sm100.so).
 
-Tolerances (relative L2 against the oracle), from the north-star contract:
+Tolerances (relative L2 against the oracle), the accuracy bar of the path:
   complex64 : 1e-6 * log2(N)
   complex128: 1e-14 * log2(N)
 """
