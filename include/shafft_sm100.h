@@ -96,8 +96,9 @@ int shafft_sm100_set_stream(shafft_sm100_plan plan, void* stream /* cudaStream_t
 
 /* Execute: src -> dst.  direction 0 = forward, 1 = backward.  The output is
  * multiplied by `scale` (pass 1.0 for the unnormalised transform).  src and
- * dst must be distinct device buffers of at least plan_elements() complex
- * elements; src's contents are undefined afterwards (it is used as
+ * dst must be distinct, 16-byte aligned device buffers (cudaMalloc memory
+ * is; others return SHAFFT_SM100_EINVAL) of at least plan_elements()
+ * complex elements; src's contents are undefined afterwards (it is used as
  * ping-pong space).  Asynchronous: enqueued on `stream` (cudaStream_t; NULL
  * selects the plan's stream). */
 int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direction, double scale,

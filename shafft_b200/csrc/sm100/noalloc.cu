@@ -184,6 +184,9 @@ extern "C" int shafft_sm100_bluestein_noalloc(const void* in, void* out, int64_t
                 (long long)n, (long long)kNoAllocMaxN);
   if (precision != 0 && precision != 1) return fail(SHAFFT_SM100_EINVAL, "bad precision");
   if (direction != 0 && direction != 1) return fail(SHAFFT_SM100_EINVAL, "bad direction");
+  const uintptr_t align = precision ? 16 : 8;  // whole complex elements
+  if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & (align - 1))
+    return fail(SHAFFT_SM100_EINVAL, "buffers must be aligned to the complex element size");
   unsigned char* base = nullptr;
   int rc = scratch_ptr(&base);
   if (rc) return rc;

@@ -1428,6 +1428,15 @@ int validate_dims(int ndim, const int64_t* dims, int precision, int64_t* total) 
 
 }  // namespace
 
+// The passes move 16-byte vectors (two complex64 or one complex128 element)
+// and bulk tensor copies need 16-byte aligned sources: a buffer that is not
+// would fault the context, so the entry points refuse it.
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+static int misaligned() {
+  return set_err(SHAFFT_SM100_EINVAL,
+                 "src and dst must be 16-byte aligned (cudaMalloc and shafftAllocBuffer memory is)");
+}
+
 namespace shafft_sm100 {
 static std::atomic<int64_t> g_tma_launches{0};
 void count_tma_launch() { g_tma_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -1529,6 +1538,7 @@ int shafft_sm100_execute(shafft_sm100_plan plan, void* src, void* dst, int direc
   if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
   if (!src || !dst) return set_err(SHAFFT_SM100_EINVAL, "null buffer");
   if (src == dst) return set_err(SHAFFT_SM100_EINVAL, "src and dst must be distinct buffers");
+  if (!aligned16(src) || !aligned16(dst)) return misaligned();
   if (direction != 0 && direction != 1) return set_err(SHAFFT_SM100_EINVAL, "bad direction");
   cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : plan->stream;
   void* bufs[4] = {src, dst, plan->d_s0, plan->d_s1};
@@ -1610,6 +1620,7 @@ int shafft_sm100_execute_step(shafft_sm100_plan plan, int step, void* src, void*
   if (!plan) return set_err(SHAFFT_SM100_EINVAL, "null plan");
   if (step < 0 || step >= (int)plan->steps.size()) return set_err(SHAFFT_SM100_EINVAL, "bad step");
   if (!src || !dst || src == dst) return set_err(SHAFFT_SM100_EINVAL, "bad buffers");
+  if (!aligned16(src) || !aligned16(dst)) return misaligned();
   cudaStream_t s = stream ? reinterpret_cast<cudaStream_t>(stream) : plan->stream;
   void* bufs[4] = {src, dst, plan->d_s0, plan->d_s1};
   return plan->precision

@@ -12,6 +12,7 @@ import pytest
 
 import shafft_b200 as S
 from oracle import oracle as o
+from shafft_b200 import _sm100
 
 pytestmark = pytest.mark.gpu
 
@@ -187,6 +188,29 @@ def test_errors_on_gpu_paths():
     assert p.plan() == S.ERR_INVALID_STATE
     assert p.execute(S.FORWARD) == S.ERR_NO_BUFFER
     assert p.normalize() == S.ERR_NO_BUFFER
+
+
+@pytest.mark.parametrize("prec", [S.C2C, S.Z2Z])
+def test_misaligned_buffers_are_refused(prec):
+    """The kernel library moves 16-byte vectors: an execute on a buffer that
+    is only element-aligned (8 bytes for complex64) or not even that is
+    refused with an error before anything is launched, and the context
+    stays usable."""
+    dims = (64, 64, 32)
+    n = math.prod(dims)
+    plan = _sm100.Plan(dims, prec, 0)
+    a, b = S.DeviceBuffer(n + 2, prec), S.DeviceBuffer(n + 2, prec)
+    for off in (8, 4):
+        with pytest.raises(_sm100.Sm100Error):
+            plan.execute(a.ptr + off, b.ptr, 0, 1.0, 0)
+        with pytest.raises(_sm100.Sm100Error):
+            plan.execute(a.ptr, b.ptr + off, 0, 1.0, 0)
+    x = o.uniform_input(dims, seed=4, dtype=np.complex128 if prec else np.complex64)
+    a.upload(x)
+    plan.execute(a.ptr, b.ptr, 0, 1.0, 0)
+    plan.status()
+    ref = o.fftn(x.astype(np.complex128), precise=bool(prec)).ravel()
+    assert o.rel_l2(b.download(n), ref) <= (1e-6 if prec == 0 else 1e-14) * math.log2(n)
 
 
 def test_set_stream():

@@ -69,6 +69,17 @@ def test_noalloc_matches_regular_entry_point_on_two_calls(prec):
         assert err <= _tol(n, prec), (call, n, err)
 
 
+def test_noalloc_rejects_misaligned_buffers():
+    f = _entry()
+    n = 1000
+    a, b = S.DeviceBuffer(n + 2, S.Z2Z), S.DeviceBuffer(n + 2, S.Z2Z)
+    assert f(a.ptr + 8, b.ptr, n, 1, 0, 1.0, None) != 0   # complex128 needs 16 bytes
+    assert f(a.ptr + 4, b.ptr, n, 0, 0, 1.0, None) != 0   # complex64 needs 8 bytes
+    assert f(a.ptr, b.ptr + 8, n, 0, 0, 1.0, None) == 0   # 8-byte aligned complex64 is fine
+    torch = pytest.importorskip("torch")
+    torch.cuda.synchronize()
+
+
 def test_noalloc_rejects_sizes_beyond_maximum():
     f = _entry()
     buf = S.DeviceBuffer(16, S.C2C)
