@@ -280,7 +280,7 @@ int tune_width(int64_t L, bool row, int64_t ext0, int default_w, size_t es, int 
     g.W = w;
     g.logW = 0;
     while ((1 << g.logW) < w) ++g.logW;
-    g.pitch = (w == 1) ? 1 : w + 1;
+    g.pitch = generic_pitch(w, row);
     if (row) {
       g.ext[0] = rows;
       g.sin[0] = g.sout[0] = L;
@@ -412,7 +412,7 @@ int batch_build(shafft_sm100_batch_s* b, int autotune) {
       g.W = W;
       g.logW = 0;
       while ((1 << g.logW) < W) ++g.logW;
-      g.pitch = (W == 1) ? 1 : W + 1;
+      g.pitch = generic_pitch(W, row);
       g.tiles_w = (g.ext[0] + W - 1) / W;
       g.ntiles = g.tiles_w * g.ext[1] * g.ext[2] * g.ext[3];
       g.in_row = row ? 1 : 0;

@@ -170,7 +170,7 @@ __device__ __forceinline__ void generic_tile(const PassGeom& g, const typename C
   const int L = LS ? LS : g.L;
   const int W = WS ? WS : g.W;
   const int logW = WS ? ilog2c(WS) : g.logW;
-  const int pitch = WS ? (WS == 1 ? 1 : WS + 1) : g.pitch;
+  const int pitch = g.pitch;  // generic_pitch(W, in_row), set by the planner
   const int nst = LS ? P.n : g.nst;
 
   int64_t rest = tile;

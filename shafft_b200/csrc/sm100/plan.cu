@@ -301,13 +301,13 @@ struct Planner {
     g.W = W;
     g.logW = 0;
     while ((1 << g.logW) < W) ++g.logW;
-    g.pitch = (W == 1) ? 1 : W + 1;
     for (int d = 0; d < 4; ++d)
       if (g.ext[d] < 1) g.ext[d] = 1;
     g.tiles_w = (g.ext[0] + W - 1) / W;
     g.ntiles = g.tiles_w * g.ext[1] * g.ext[2] * g.ext[3];
     g.in_row = (g.sn_in == 1) ? 1 : 0;
     g.out_row = (g.sk_out == 1) ? 1 : 0;
+    g.pitch = generic_pitch(W, g.in_row != 0);
     g.scale = 1.0;
     st.smem = (size_t)g.L * (size_t)g.pitch * elem;
     st.tabL = ltab(g.L);
