@@ -220,3 +220,22 @@ def test_measured_plan_query_uses_cached_choice(tmp_path, monkeypatch):
     cache.write_text("c64:f0:m18446744073709551615:16777216 0 1 -1\n")
     assert lens(_sm100.plan_query([1 << 24], 0, M)) == [16, 1024, 1024]
     assert lens(_sm100.plan_query([1 << 24], 0)) == [256, 256, 256]
+
+
+@pytest.mark.parametrize("dims,prec", [((1488375,), 0), ((1488375,), 1), ((4096, 97), 0), ((512, 45, 45), 0),
+                                       ((2048, 33), 0), ((35, 27, 45), 0)])
+def test_generic_pass_tile_pitch_rule(dims, prec):
+    """Generic passes size their shared-memory tile [L][pitch] with pitch W
+    for column input and for row input of W <= 4, and W + 1 for row input of
+    W >= 8 (bank-conflict rule of generic_pitch in the kernel library)."""
+    q = _sm100.plan_query(dims, prec, 0)
+    es = 16 if prec else 8
+    seen = 0
+    for s in q["steps"]:
+        if s["kind"] != "pass" or s.get("fast") or s.get("tc"):
+            continue
+        W = s["W"]
+        want = 1 if W == 1 else (W + 1 if (s["in_row"] and W >= 8) else W)
+        assert s["smem"] == s["L"] * want * es, s
+        seen += 1
+    assert seen
