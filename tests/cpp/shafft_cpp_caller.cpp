@@ -46,6 +46,12 @@ int main() {
           "execute after init, before plan");
     MPI_Comm c = MPI_COMM_NULL;
     check(p.getCommunicator(&c) == 0 && c != MPI_COMM_NULL, "communicator available after init");
+    // an active rank must hand over both buffers (src/cpp/shafft_internal.cpp:505-523)
+    check(p.setBuffersRaw(nullptr, nullptr) == st(Status::ERR_NULLPTR), "null buffers on an active rank");
+    void* d = nullptr;
+    void* w = nullptr;
+    check(p.getBuffersRaw(&d, &w) == st(Status::ERR_NO_BUFFER) && !d && !w,
+          "getBuffers on an active rank without buffers");
 
     // move construction and assignment leave the source uninitialised
     FFTND q(std::move(p));
@@ -60,6 +66,13 @@ int main() {
     r.release();  // idempotent
     check(!r.isConfigured(), "double release is safe");
     check(r.init({1, 1}, {16, 16}, FFTType::Z2Z, MPI_COMM_WORLD) == 0, "init again after release");
+  }
+
+  {  // an inactive rank (MPI_COMM_NULL) owns nothing and may pass null buffers
+    FFTND p;
+    check(p.init({1, 1}, {8, 8}, FFTType::C2C, MPI_COMM_NULL) == 0 && !p.isActive() && p.allocSize() == 0,
+          "inactive rank");
+    check(p.setBuffersRaw(nullptr, nullptr) == 0, "inactive rank accepts null buffers");
   }
 
   {  // FFTND argument errors
