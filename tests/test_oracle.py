@@ -88,3 +88,17 @@ def test_norm_factors_follow_reference():
     assert o.nd_norm_factor(512 ** 3, 1) == pytest.approx(1 / np.sqrt(512.0 ** 3), rel=1e-15)
     assert o.fft1d_norm_factor(1000003, 1, double=False) == float(np.float32(1) / np.sqrt(np.float32(1000003)))
     assert o.nd_norm_factor(100, 0) == 1.0
+
+
+@pytest.mark.parametrize("dims", [(2, 3, 2, 2, 3, 2, 2, 2), (2,) * 9, (3, 2, 2, 2, 2, 2, 2, 2, 2, 2),
+                                  (2,) * 11, (2,) * 12])
+def test_high_rank_tensors_vs_naive_dft(dims):
+    """8-D to 12-D tensors against the naive DFT, as the reference's
+    high-dimensional unit tests do (tests/unit/test_fft_highdim.cpp:186-205):
+    the oracle's FFT and its naive DFT agree to FP64 rounding, forward and
+    backward."""
+    x = o.uniform_input(dims, seed=len(dims), dtype=np.complex128)
+    for sign in (-1, 1):
+        y = o.fftn(x, sign=sign)
+        ref = o.naive_dft(x, sign=sign)
+        assert o.rel_l2(y, ref) <= 1e-13, (dims, sign)
