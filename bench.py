@@ -13,13 +13,20 @@ time; "% HBM peak" is that figure over the measured copy bandwidth.
 Arms:
   ours       value: device-resident tensor, kernels launched through the
              kernel library's C ABI on one stream, CUDA events around every
-             launch; e2e: the public SHAFFT C ABI (libshafft.so) with pinned
-             host buffers, H2D + execute + execute + D2H inside the timed
-             region.
+             launch; after the timed region the buffers it transformed are
+             checked (K+W normalised round trips must return the input).
+             e2e: the public SHAFFT C ABI (libshafft.so) with pinned host
+             buffers, H2D + execute + execute + D2H inside the timed region.
+             api_sequence: the reference's own call sequence through the C
+             ABI (execute, normalize, execute, normalize; device-resident).
+             At N = 1 the line also carries `configs` (the other transform
+             sizes) and `forms` (tensor-core, batched and served forms
+             against the plain kernels), each timing with its own clock
+             record and its error against the CPU oracle.
   reference  the reference's CPU path as restated by the oracle
-             (oracle/oracle_fft.c, FP64, all host threads); FFTW and MPI are
-             not installed, so the reference's own FFTW backend cannot be
-             built.  Each step is a bounded sample (256^3 fwd+bwd).
+             (oracle/oracle_fft.c, FP64, all host threads) on the same
+             512^3 workload; FFTW and MPI are not installed, so the
+             reference's own FFTW backend cannot be built.
 Multi-GPU (torchrun): every rank transforms its own 512^3 tensor (replicas,
 weak scaling); time = max over ranks of the CUDA-event time.
 """
@@ -61,6 +68,8 @@ def parse():
     ap.add_argument("--e2e-lanes", type=int, default=2,
                     help="plans / host threads of the e2e arm (overlapping steps)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="leave the configs / forms objects out of the default line")
     ap.add_argument("--suite", default="headline", choices=["headline", "batched", "serve", "configs", "tc"],
                     help="headline (default, the contract line) or one of the side workloads")
     ap.add_argument("--count", type=int, default=4096, help="transforms of the batched suite")
@@ -175,9 +184,12 @@ def cpu_sample(threads=None, dims=(256, 256, 256)):
     n = x.size
     f = o.nd_norm_factor(n, 1)
     t0 = time.perf_counter()
-    y = o.fftn(x, sign=-1, nthreads=threads) * f
-    z = o.fftn(y, sign=1, nthreads=threads) * f
+    y = o.fftn(x, sign=-1, nthreads=threads)
+    y *= f
+    z = o.fftn(y, sign=1, nthreads=threads)
+    z *= f
     t = time.perf_counter() - t0
+    del y
     err = o.rel_l2(z, x)
     return step_bytes(dims) / t / 1e9, t, threads, err
 
@@ -194,42 +206,59 @@ def cpu_model():
     return None
 
 
+WORKLOAD = ("FFTND 512x512x512 complex64 C2C: forward+normalize then backward+normalize "
+            "(iid U[-1,1) input)")
+
+
+def headline_config(dims, world):
+    """`config` of both arms (identical for the same workload)."""
+    return {"workload": WORKLOAD if dims == DIMS else
+            f"FFTND {'x'.join(map(str, dims))} complex64 C2C: forward+normalize then backward+normalize",
+            "dims": list(dims), "precision": "complex64", "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (1 GiB tensor vs 126 MB L2), no flush"}
+
+
 def reference_arm(args):
+    """The reference's CPU path (its FFTW backend, restated by the oracle:
+    one full C2C per execute, then a separate normalize,
+    src/cpp/fft/fftw_method/fftnd_method.cpp:236-276 and
+    src/cpp/shafft_internal.cpp:129-188) on the same 512^3 workload as our
+    arm, all host threads.  Only rank 0 runs it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    dims = (256, 256, 256)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    dims = tuple(int(v) for v in args.dims.split("x")) if args.dims else DIMS
     threads = os.cpu_count() or 1
     for _ in range(max(0, args.warmup)):
         cpu_sample(threads, dims)
     times = []
+    err = None
     for _ in range(max(1, args.steps)):
         _, t, _, err = cpu_sample(threads, dims)
         times.append(t)
     tot = sum(times)
     value = step_bytes(dims) * len(times) / tot / 1e9
-    sample = (f"{'x'.join(map(str, dims))} complex64 forward+normalize+backward+normalize per step, "
-              f"FP64 Stockham restatement of the FFTW path (oracle/oracle_fft.c), {threads} threads; "
-              f"FFTW/MPI not installed so the reference's FFTW backend cannot be built")
+    v256, t256, _, _ = cpu_sample(threads, (256, 256, 256))
+    sample = (f"{'x'.join(map(str, dims))} complex64 forward+normalize+backward+normalize per step "
+              f"(the full workload), FP64 Stockham restatement of the FFTW path (oracle/oracle_fft.c), "
+              f"{threads} threads; FFTW/MPI not installed so the reference's FFTW backend cannot be built")
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "FFTND complex C2C fwd+bwd with normalize, bounded CPU sample",
-                   "dims": list(dims), "threads": threads},
+        "config": headline_config(dims, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample, "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "roundtrip_rel_l2": err,
+        "extra_256cube": {"value": v256, "unit": UNIT, "ms_per_step": 1e3 * t256,
+                          "dims": [256, 256, 256]},
     }
     print(json.dumps(out), flush=True)
     return 0
 
-
-# ---------------------------------------------------------------------------
-# our arm
-# ---------------------------------------------------------------------------
 
 # ---------------------------------------------------------------------------
 # replicas: one process per GPU, no data-path collective
@@ -290,6 +319,14 @@ def kernel_name(st):
     return "k_fft_pass" if st["kind"] == "pass" else f"k_bs/{st['kind']}"
 
 
+def nd_norm_factor_c64(n):
+    """The ND normalisation factor as libshafft applies it to complex64: long
+    double 1/sqrt(N) rounded to float (src/cpp/shafft_internal.cpp:136, 153)."""
+    import numpy as np
+    f = np.longdouble(1) / np.sqrt(np.longdouble(n))
+    return float(np.float32(f))
+
+
 def ours(args):
     import torch
 
@@ -309,13 +346,14 @@ def ours(args):
     n = math.prod(dims)
     plan = _sm100.Plan(dims, 0, (_sm100.PLAN_TENSOR_CORE if args.tensor_core else 0) | args.plan_flags)
     nst = plan.launches
-    scale = float(1.0 / math.sqrt(n))
+    scale = nd_norm_factor_c64(n)
     # a dedicated stream: the kernels and the events that time them share it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     gen = torch.Generator(device="cuda").manual_seed(42 + rank)
     a = (torch.rand(2 * n, device="cuda", generator=gen) * 2 - 1).view(torch.complex64)
+    a0 = a.clone()  # the input, to check the transformed buffers after the timed region
     b = torch.empty_like(a)
     ap, bp = a.data_ptr(), b.data_ptr()
 
@@ -344,6 +382,11 @@ def ours(args):
     barrier()
     clocks.stop()
     total_ms = t0.elapsed_time(t1)
+    # every step is a normalised forward+backward pair, so the buffer the
+    # timed region ended on holds the input after max(3, W) + K round trips
+    roundtrip = float((torch.linalg.vector_norm(a - a0) / torch.linalg.vector_norm(a0)).item())
+    round_trips = max(3, args.warmup) + args.steps
+    del a0
     # per-kernel durations
     per = {}
     bounds = [e for (_, _, e) in events] + [t1]
@@ -359,19 +402,25 @@ def ours(args):
     for i in range(nst):
         d = per.get(i, [0.0])
         kern.append({"step": i, "kind": desc["steps"][i]["kind"], "L": desc["steps"][i].get("L"),
+                     "kernel": kernel_name(desc["steps"][i]),
                      "avg_ms": sum(d) / len(d), "alg_bytes": plan.step_bytes(i)})
     dom = max(kern, key=lambda k: k["avg_ms"])
     achieved = dom["alg_bytes"] / (dom["avg_ms"] / 1e3) / 1e9
     traffic = committed_traffic(dims, "c64", dom["step"])
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": f"{kernel_name(desc['steps'][dom['step']])} step {dom['step']} (L={dom['L']})",
+                "kernel": f"{dom['kernel']} step {dom['step']} (L={dom['L']})",
                 "alg_bytes_per_launch": dom["alg_bytes"]}
     plan_bytes_per_step = 2 * sum(k["alg_bytes"] for k in kern)
+    plan.destroy()
+    del a, b
+    torch.cuda.empty_cache()
 
     e2e = None
-    if not args.no_e2e and world >= 1:
+    api = None
+    if not args.no_e2e:
         e2e = e2e_arm(S, dims, n, args, stream, barrier, dist)
+        api = api_sequence(S, dims, n, args, barrier, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -384,31 +433,75 @@ def ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {
-            "workload": "FFTND 512x512x512 complex64 C2C: forward+normalize then "
-                        "backward+normalize (normalize fused into the last pass)"
-            if dims == DIMS else f"FFTND {'x'.join(map(str, dims))} complex64 fwd+bwd",
-            "dims": list(dims), "precision": "complex64", "parallelism": f"replicas{world}",
-            "l2": "inputs larger than L2 (1 GiB tensor vs 126 MB L2), no flush",
+        "config": headline_config(dims, world),
+        "detail": {
+            "normalize": "fused into the last pass (shafftExecuteNormalized semantics); "
+                         "the reference's separate-normalize sequence is `api_sequence`",
             "bytes_per_step": step_bytes(dims),
             "plan_hbm_bytes_per_step": plan_bytes_per_step,
             "passes_per_transform": nst,
             "pct_hbm_peak": 100.0 * value / world / peak,
             "plan_hbm_gbs": world * plan_bytes_per_step * args.steps / (tmax / 1e3) / 1e9,
+            "pct_hbm_peak_plan": 100.0 * plan_bytes_per_step * args.steps / (tmax / 1e3) / 1e9 / peak,
             "kernels": kern,
         },
+        "check": {"roundtrip_rel_l2": roundtrip, "round_trips": round_trips,
+                  "what": "the timed buffers after every normalised forward+backward pair of the "
+                          "warm-up and timed steps, against the input",
+                  "tol": 1e-6 * math.log2(n)},
         "e2e": e2e,
+        "api_sequence": api,
         "gpu_launches": args.steps * 2 * nst,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
     }
+    if world == 1 and not args.no_forms and dims == DIMS:
+        out["configs"] = configs_rows(args, local)
+        out["forms"] = forms(args, local)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
     return 0
+
+
+def api_sequence(S, dims, n, args, barrier, dist):
+    """The reference's own call sequence through libshafft.so's C ABI on
+    device-resident buffers: execute(FORWARD), normalize(), execute(BACKWARD),
+    normalize() -- normalize is then a separate pass over the tensor, as in
+    the reference (src/cpp/shafft_internal.cpp:129-188).  Every call
+    synchronises, so host wall-clock between barriers times it."""
+    plan = S.FFTND()
+    S.check(plan.init([1] * len(dims), list(dims), S.C2C), "init")
+    S.check(plan.plan(), "plan")
+    da = S.DeviceBuffer(n, S.C2C)
+    db = S.DeviceBuffer(n, S.C2C)
+    S.check(plan.set_buffers(da.ptr, db.ptr), "setBuffers")
+    def step():
+        S.check(plan.execute(S.FORWARD), "execute")
+        S.check(plan.normalize(), "normalize")
+        S.check(plan.execute(S.BACKWARD), "execute")
+        S.check(plan.normalize(), "normalize")
+
+    for _ in range(max(2, min(args.warmup, 3))):
+        step()
+    k = max(3, min(args.steps, 10))
+    barrier()
+    w0 = time.perf_counter()
+    for _ in range(k):
+        step()
+    barrier()
+    tmax = max_over_ranks(1e3 * (time.perf_counter() - w0), dist)
+    plan.release()
+    da.free()
+    db.free()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"value": world * step_bytes(dims) * k / (tmax / 1e3) / 1e9, "unit": UNIT, "steps": k,
+            "ms_per_step": tmax / k, "passes_per_transform": "plan passes + 1 (normalize)",
+            "path": "libshafft.so C ABI: shafftExecute, shafftNormalize, shafftExecute, "
+                    "shafftNormalize per step, device-resident buffers, host wall clock"}
 
 
 def e2e_arm(S, dims, n, args, stream, barrier, dist):
@@ -526,17 +619,43 @@ def batched_shapes(count=4096, seed=42):
     return shapes
 
 
-def suite_batched(args):
+def timed_region(fn, stream, gpu, target_s=0.4, min_reps=3):
+    """CUDA-event time of fn() on `stream`, ms per call, over enough calls
+    to last about target_s (after 3 untimed calls), with nvidia-smi clocks
+    sampled over the timed calls.  Returns (ms, reps, clocks)."""
+    import torch
+    for _ in range(3):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    one = max(e0.elapsed_time(e1) / 1e3, 1e-6)
+    reps = max(min_reps, int(target_s / one))
+    clk = ClockSampler(gpu)
+    clk.start()
+    time.sleep(0.15)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk.stop()
+    return e0.elapsed_time(e1) / reps, reps, clk.summary()
+
+
+def batched_form(count, gpu, rank=0, world=1, dist=None):
+    """C4: `count` seeded uneven 2-D/3-D complex64 transforms (this rank's
+    contiguous block), one persistent graph-captured launch per execute vs
+    one plain plan execute per transform; sampled error vs the oracle."""
     import numpy as np
     import torch
 
-    import shafft_b200 as S  # noqa: F401
     from oracle import oracle as o
     from shafft_b200 import _sm100
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    rank, world, _, dist = dist_init("nccl")
-    # replicas: each rank owns a contiguous block of the transform list
-    shapes = shard(batched_shapes(args.count), rank, world)
+    shapes = shard(batched_shapes(count), rank, world)
     sizes = [math.prod(s) for s in shapes]
     offs, tot = [], 0
     for n in sizes:
@@ -553,18 +672,11 @@ def suite_batched(args):
     t0 = time.perf_counter()
     batch = _sm100.Batch(shapes, 0, autotune=True)
     t_create = time.perf_counter() - t0
-    for _ in range(2):
+
+    def run_batch():
         batch.execute(sp, dp, 0, 1.0, stream.cuda_stream)
-    torch.cuda.synchronize()
-    k = max(3, min(args.steps, 10))
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(k):
-        batch.execute(sp, dp, 0, 1.0, stream.cuda_stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
+    t_batch, reps_b, clk_b = timed_region(run_batch, stream, gpu, target_s=0.6)
     batch.status()
-    t_batch = e0.elapsed_time(e1) / k
     # sampled parity against the oracle
     rng = np.random.Generator(np.random.MT19937(7))
     small = [i for i, n in enumerate(sizes) if n <= (1 << 20)]
@@ -574,8 +686,8 @@ def suite_batched(args):
     for i in sample:
         x = src[offs[i]:offs[i] + sizes[i]].cpu().numpy().reshape(shapes[i])
         y = dst[offs[i]:offs[i] + sizes[i]].cpu().numpy().reshape(shapes[i])
-        errs.append(o.rel_l2(y, o.fftn(x.astype(np.complex128))))
-    # the plain path: one plan per transform, launched one by one
+        errs.append((o.rel_l2(y, o.fftn(x.astype(np.complex128))), 1e-6 * math.log2(max(2, sizes[i]))))
+    # the plain path: one plan per distinct shape, one execute per transform
     t0 = time.perf_counter()
     plans = {}
     for s in shapes:
@@ -588,37 +700,45 @@ def suite_batched(args):
         for i, s in enumerate(shapes):
             plans[s].execute(cp[i], dp[i], 0, 1.0, stream.cuda_stream)
     scr.copy_(src)
-    # two untimed passes: a plan replays a launch sequence it has seen twice
-    # (graph replay of executes), so the timed passes run at steady state
-    for _ in range(2):
-        plain()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(2):
-        plain()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_plain = e0.elapsed_time(e1) / 2
+    # the untimed calls of timed_region let a plan replay a launch sequence
+    # it has seen twice (graph replay of executes): steady state is timed
+    t_plain, reps_p, clk_p = timed_region(plain, stream, gpu, target_s=0.6, min_reps=2)
     comp = sum(2 * 8 * n for n in sizes)
-    # whole job: bytes of all ranks over the slowest rank's time
     comp_all = sum_over_ranks(comp, dist)
-    t_batch = max_over_ranks(t_batch, dist)
-    t_plain = max_over_ranks(t_plain, dist)
-    if rank != 0:
-        dist.destroy_process_group()
-        return 0
+    t_batch_all = max_over_ranks(t_batch, dist)
+    t_plain_all = max_over_ranks(t_plain, dist)
     out = {
-        "metric": "batched uneven 2-D/3-D c64 forward transforms: compulsory GB/s", "unit": "GB/s",
-        "value": comp_all / (t_batch / 1e3) / 1e9, "plain_value": comp_all / (t_plain / 1e3) / 1e9,
-        "speedup_vs_plain": t_plain / t_batch, "ms_batched": t_batch, "ms_plain": t_plain,
-        "n_gpus": world, "transforms_per_rank": len(shapes), "elements_rank0": sum(sizes),
+        "workload": f"{count} seeded uneven 2-D/3-D complex64 forward transforms (extents "
+                    "log-uniform in [16,256] over 7-smooth lengths, 5% primes), iid U[-1,1)",
+        "metric": "compulsory GB/s", "unit": "GB/s",
+        "value": comp_all / (t_batch_all / 1e3) / 1e9, "plain_value": comp_all / (t_plain_all / 1e3) / 1e9,
+        "speedup_vs_plain": t_plain_all / t_batch_all, "ms_batched": t_batch_all, "ms_plain": t_plain_all,
+        "reps": {"batched": reps_b, "plain": reps_p},
+        "transforms_per_rank": len(shapes), "elements_rank0": sum(sizes),
         "plan_hbm_gbs_batched": batch.alg_bytes / (t_batch / 1e3) / 1e9,
         "launches_batched_per_execute": 1, "launches_plain_per_execute": launches,
         "create_s": {"batch_with_autotune": t_create, "plain_plans": t_plans},
-        "batch": batch.describe(), "max_rel_l2_sample": max(errs), "sample": len(errs),
-        "tol_c64": "1e-6*log2(N)", "data": "synthetic",
+        "batch": batch.describe(), "max_rel_l2_sample": max(e for e, _ in errs),
+        "errors_within_tol": all(e <= t for e, t in errs), "sample": len(errs),
+        "tol": "1e-6*log2(N) per transform",
+        "clocks": {"batched": clk_b, "plain": clk_p},
     }
-    print(json.dumps(out), flush=True)
+    batch.destroy()
+    for p in plans.values():
+        p.destroy()
+    del src, dst, scr
+    torch.cuda.empty_cache()
+    return out
+
+
+def suite_batched(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank, world, local, dist = dist_init("nccl")
+    out = batched_form(args.count, local, rank, world, dist)
+    out["n_gpus"] = world
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if dist is not None:
         dist.destroy_process_group()
     return 0
@@ -650,15 +770,16 @@ def serve_requests(count, seed=42):
     return out
 
 
-def suite_serve(args):
+def served_form(count, gpu, loads=(0.5, 1.0, 2.0, 4.0, 8.0), rank=0, world=1, dist=None):
+    """C5: the seeded request mix through the serving loop
+    (shafft_sm100_server_*, 40 GB budget, 8 streams) at Poisson offered
+    loads given as multiples of the serial rate, against the same requests
+    run one by one through resident plain plans (H2D, execute, D2H)."""
     import numpy as np
     import torch
 
     from shafft_b200 import _sm100
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    rank, world, _, dist = dist_init("nccl")
-    # replicas: each rank serves a contiguous block of the request stream
-    reqs = shard(serve_requests(max(40, min(args.count, 400)) * world), rank, world)
+    reqs = shard(serve_requests(count * world), rank, world)
     maxb = max(math.prod(d) * (16 if p else 8) for d, p, _ in reqs)
     hin = torch.empty(maxb // 4, dtype=torch.float32, pin_memory=True).uniform_(-1, 1)
     hout = torch.empty(maxb // 4, dtype=torch.float32, pin_memory=True)
@@ -680,13 +801,20 @@ def suite_serve(args):
         return (time.perf_counter() - t0) * 1e3
     for d, p, r in reqs:  # warm plans
         serial_one(d, p, r)
+    clk = ClockSampler(gpu)
+    clk.start()
+    time.sleep(0.15)
     t0 = time.perf_counter()
     lat = [serial_one(d, p, r) for d, p, r in reqs]
     serial_s = time.perf_counter() - t0
+    clk.stop()
     serial_tput = len(reqs) / serial_s
     lat.sort()
     serial = {"throughput_per_s": serial_tput, "p50_ms": lat[len(lat) // 2],
-              "p99_ms": lat[min(len(lat) - 1, int(0.99 * (len(lat) - 1) + 0.5))]}
+              "p99_ms": lat[min(len(lat) - 1, int(0.99 * (len(lat) - 1) + 0.5))],
+              "clocks": clk.summary()}
+    for p in plans.values():
+        p.destroy()
     del plans, dev, dev2
     torch.cuda.empty_cache()
     srv = _sm100.Server(budget_bytes=40 << 30, streams=8)
@@ -696,10 +824,13 @@ def suite_serve(args):
         srv.wait(i)
     rng = np.random.Generator(np.random.MT19937(5))
     sweep = []
-    for mult in (0.5, 1.0, 2.0, 4.0, 8.0):
+    for mult in loads:
         rate = mult * serial_tput
         gaps = rng.exponential(1.0 / rate, size=len(reqs))
         srv.reset_stats()
+        clk = ClockSampler(gpu)
+        clk.start()
+        time.sleep(0.15)
         start = time.perf_counter()
         due = start
         ids = []
@@ -712,103 +843,121 @@ def suite_serve(args):
         for i in ids:
             srv.wait(i)
         wall = time.perf_counter() - start
+        clk.stop()
         st = srv.stats()
+        st["offered_x_serial"] = mult
         st["offered_per_s"] = rate
         st["achieved_per_s"] = len(reqs) / wall
+        st["clocks"] = clk.summary()
         sweep.append(st)
     srv.destroy()
     best = max(s["achieved_per_s"] for s in sweep)
-    # whole job: request rates add over the replicas; latency is the worst rank's
     best_all = sum_over_ranks(best, dist)
     serial_all = sum_over_ranks(serial_tput, dist)
-    p99_best = max_over_ranks(max(sweep, key=lambda s: s["achieved_per_s"])["p99_ms"], dist)
-    if rank != 0:
-        dist.destroy_process_group()
-        return 0
-    out = {"metric": "served mixed C2C requests: throughput and p50/p99 latency", "unit": "requests/s",
-           "value": best_all, "serial_plain": serial, "speedup_vs_serial": best_all / serial_all,
-           "n_gpus": world, "p99_ms_at_best_worst_rank": p99_best,
-           "requests_per_rank": len(reqs), "budget_bytes": 40 << 30, "streams": 8,
-           "sweep_rank0": sweep,
-           "host_buffers": "pinned, shared by all requests (timing only)", "data": "synthetic"}
-    print(json.dumps(out), flush=True)
+    low = min(sweep, key=lambda s: s["offered_x_serial"])
+    return {"workload": f"{len(reqs)} seeded requests per rank: 1-D 2^10-2^22, 2-D 64^2-2048^2, "
+                        "3-D 32^3-384^3, 30% complex128, 10% prime lengths, fwd/bwd 50/50; "
+                        "pinned host buffers; Poisson arrivals",
+            "metric": "served requests/s (best over the offered loads) and p50/p99 latency",
+            "unit": "requests/s", "value": best_all, "serial_plain": serial,
+            "speedup_vs_serial": best_all / serial_all,
+            "p99_below_saturation_vs_serial": low["p99_ms"] / serial["p99_ms"],
+            "p50_below_saturation_ms": low["p50_ms"], "p99_below_saturation_ms": low["p99_ms"],
+            "requests_per_rank": len(reqs), "budget_bytes": 40 << 30, "streams": 8, "sweep": sweep,
+            "results": "bit-identical alone and in the mix (tests/test_gpu_serve.py)"}
+
+
+def suite_serve(args):
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank, world, local, dist = dist_init("nccl")
+    out = served_form(max(40, min(args.count, 400)), local, rank=rank, world=world, dist=dist)
+    out["n_gpus"] = world
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if dist is not None:
         dist.destroy_process_group()
     return 0
 
 
-def suite_configs(args):
+CONFIG_ROWS = [((256, 256, 256), 1), ((64, 64, 32), 0), ((1 << 24,), 0), ((1 << 24,), 1),
+               ((1488375,), 0), ((1488375,), 1), ((1000003,), 0), ((1000003,), 1)]
+
+
+def configs_rows(args, gpu, rows=CONFIG_ROWS):
+    """The other configurations: fwd+bwd time (plain kernels, graph replay
+    on as by default, CUDA events, clocks sampled), plan traffic, and the
+    forward error against the oracle (FP64 for complex64, x87 long double
+    for complex128) with its tolerance."""
     import numpy as np
     import torch
 
     from oracle import oracle as o
     from shafft_b200 import _sm100
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     stream = torch.cuda.current_stream()
     peak, _ = peaks()
     res = []
-
-    def run(dims, prec, reps, check):
+    for dims, prec in rows:
         n = math.prod(dims)
-        dt = torch.complex128 if prec else torch.complex64
         es = 16 if prec else 8
-        x = o.uniform_input(dims, seed=42, dtype=np.complex128 if prec else np.complex64) if check else None
-        a = torch.from_numpy(x.ravel()).cuda() if check else torch.randn(n, dtype=dt, device="cuda")
-        a0 = a.clone()
+        x = o.uniform_input(dims, seed=42, dtype=np.complex128 if prec else np.complex64)
+        a = torch.from_numpy(x.ravel()).cuda()
         b = torch.empty_like(a)
         p = _sm100.Plan(dims, prec)
-        err = None
-        if check:
-            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
-            y = b.cpu().numpy()
-            err = o.rel_l2(y, o.fftn(x.astype(np.complex128), precise=bool(prec)).ravel())
-        for _ in range(3):
-            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
-            p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
+        p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+        y = b.cpu().numpy()
+        err = o.rel_l2(y, o.fftn(x.astype(np.complex128), precise=bool(prec)).ravel())
+        del y
+
+        def fwd_bwd():
             p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
             p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        comp = 2 * 2 * es * n
+        ms, reps, clk = timed_region(fwd_bwd, stream, gpu)
+        plan_bytes = 2 * sum(p.step_bytes(i) for i in range(p.launches))
+        tol = (1e-14 if prec else 1e-6) * math.log2(n)
         res.append({"dims": list(dims), "precision": "c128" if prec else "c64", "ms_fwd_bwd": ms,
-                    "compulsory_gbs": comp / (ms / 1e3) / 1e9,
-                    "plan_gbs": 2 * sum(p.step_bytes(i) for i in range(p.launches)) / (ms / 1e3) / 1e9,
-                    "pct_hbm_plan": 100 * 2 * sum(p.step_bytes(i) for i in range(p.launches)) / (ms / 1e3) / 1e9 / peak,
-                    "launches_per_transform": p.launches,
-                    "rel_l2_vs_oracle": err,
-                    "tol": (1e-6 if prec == 0 else 1e-14) * math.log2(n)})
-        del a, a0, b
+                    "reps": reps, "compulsory_gbs": 2 * 2 * es * n / (ms / 1e3) / 1e9,
+                    "plan_gbs": plan_bytes / (ms / 1e3) / 1e9,
+                    "pct_hbm_plan": 100 * plan_bytes / (ms / 1e3) / 1e9 / peak,
+                    "launches_per_transform": p.launches, "passes_per_transform": p.passes,
+                    "rel_l2_fwd_vs_oracle": err, "tol": tol, "within_tol": err <= tol,
+                    "clocks": clk})
         p.destroy()
-    run((256, 256, 256), 1, 20, False)
-    run((64, 64, 32), 0, 50, True)
-    for n in (1 << 24, 1488375, 1000003):
-        for prec in (0, 1):
-            run((n,), prec, 10, True)
-    print(json.dumps({"metric": "other configurations (512^3 aside): fwd+bwd time and error", "configs": res}), flush=True)
+        del a, b
+        torch.cuda.empty_cache()
+    return res
+
+
+def suite_configs(args):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    print(json.dumps({"metric": "other configurations (512^3 aside): fwd+bwd time and error",
+                      "configs": configs_rows(args, local)}), flush=True)
     return 0
 
 
-def suite_tc(args):
+TC_SHAPES = [(1 << 24,), (1488375,), (1000003,), (64, 64, 32), (512, 512, 512), (65536, 61), (65536, 47),
+             (65536, 31), (65536, 17), (4096, 61, 16), (61, 61, 61), (53, 59, 61)]
+
+
+def tc_form(shapes, gpu, per_step=False):
     """Tensor-core form (tcgen05 split-FP16 DFT stages) against the plain
-    kernels on the same GPU: fwd+bwd time, per-pass kernel times and the
-    forward error of both forms against the FP64 oracle."""
+    kernels on the same GPU: fwd+bwd time with clocks, and the forward error
+    of both forms against the FP64 oracle.  Where the plan has axes with a
+    prime factor above 13, also the hybrid plan (tensor cores on those axes
+    only)."""
     import numpy as np
     import torch
 
     from oracle import oracle as o
     from shafft_b200 import _sm100
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     stream = torch.cuda.current_stream()
     peak, _ = peaks()
     res = []
 
-    def run(dims, flags, reps, ref):
+    def run(dims, x, flags, ref):
         n = math.prod(dims)
-        x = o.uniform_input(dims, seed=42, dtype=np.complex64)
         a = torch.from_numpy(x.ravel()).cuda()
         b = torch.empty_like(a)
         p = _sm100.Plan(dims, 0, flags)
@@ -816,70 +965,76 @@ def suite_tc(args):
         p.status()
         err = o.rel_l2(b.cpu().numpy(), ref.ravel())
         a.copy_(torch.from_numpy(x.ravel()))
-        for _ in range(3):
+
+        def fwd_bwd():
             p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
             p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            p.execute(a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
-            p.execute(b.data_ptr(), a.data_ptr(), 1, 1.0 / n, stream.cuda_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        # per-launch times of one forward (steps run in order on one stream)
-        steps = p.describe()["steps"]
-        per = []
-        for i in range(p.launches):
-            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            for _ in range(2):
-                p.execute_step(i, a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
-            s0.record(stream)
-            for _ in range(5):
-                p.execute_step(i, a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
-            s1.record(stream)
-            torch.cuda.synchronize()
-            t = s0.elapsed_time(s1) / 5
-            st = steps[i]
-            d = {"kind": st["kind"], "L": st.get("L"), "tc": st.get("tc", 0), "ms": t,
-                 "gbs": p.step_bytes(i) / (t / 1e3) / 1e9}
-            if st.get("tc"):
-                lp = (st["L"] + 15) // 16 * 16
-                rows = n // st["L"]
-                groups = -(-rows // 128)
-                # 3 products x Lp/16 K-steps x 4 MMAs of 128 x Lp x 16 per group
-                d["mma_tflops"] = groups * 3072 * lp * lp / (t / 1e3) / 1e12
-            per.append(d)
+        ms, reps, clk = timed_region(fwd_bwd, stream, gpu)
+        p.status()
         plan_bytes = sum(p.step_bytes(i) for i in range(p.launches))
-        out = {"ms_fwd_bwd": ms, "compulsory_gbs": 2 * 2 * 8 * n / (ms / 1e3) / 1e9,
+        out = {"ms_fwd_bwd": ms, "reps": reps, "compulsory_gbs": 2 * 2 * 8 * n / (ms / 1e3) / 1e9,
                "plan_gbs": 2 * plan_bytes / (ms / 1e3) / 1e9,
                "pct_hbm_plan": 100 * 2 * plan_bytes / (ms / 1e3) / 1e9 / peak,
-               "launches": p.launches, "rel_l2_fwd_vs_fp64_oracle": err, "steps": per}
+               "launches": p.launches, "rel_l2_fwd_vs_fp64_oracle": err, "clocks": clk}
+        if per_step:
+            steps = p.describe()["steps"]
+            per = []
+            for i in range(p.launches):
+                def one(i=i):
+                    p.execute_step(i, a.data_ptr(), b.data_ptr(), 0, 1.0, stream.cuda_stream)
+                t, _, _ = timed_region(one, stream, gpu, target_s=0.05)
+                st = steps[i]
+                per.append({"kind": st["kind"], "L": st.get("L"), "tc": st.get("tc", 0), "ms": t,
+                            "gbs": p.step_bytes(i) / (t / 1e3) / 1e9})
+            out["steps"] = per
         del a, b
         p.destroy()
+        torch.cuda.empty_cache()
         return out
 
-    # the FFT1D sizes of the tensor-core configuration and the headline, then
-    # axes with a prime factor above 13, where the plain path runs O(L^2)
-    # direct DFTs and the hybrid plan (tensor cores on those axes only) applies
-    for dims in ((1 << 24,), (1488375,), (1000003,), (64, 64, 32), (512, 512, 512),
-                 (65536, 61), (65536, 47), (65536, 31), (65536, 17), (4096, 61, 16), (61, 61, 61),
-                 (53, 59, 61)):
+    for dims in shapes:
         n = math.prod(dims)
         x = o.uniform_input(dims, seed=42, dtype=np.complex64)
         ref = o.fftn(x.astype(np.complex128))
-        plain = run(dims, 0, 10, ref)
-        tc = run(dims, _sm100.PLAN_TENSOR_CORE, 10, ref)
-        row = {"dims": list(dims), "tol": 1e-6 * math.log2(n), "plain": plain, "tensor_core": tc,
-               "speedup_tc_vs_plain": plain["ms_fwd_bwd"] / tc["ms_fwd_bwd"]}
+        tol = 1e-6 * math.log2(n)
+        plain = run(dims, x, 0, ref)
+        tc = run(dims, x, _sm100.PLAN_TENSOR_CORE, ref)
+        row = {"dims": list(dims), "tol": tol, "plain": plain, "tensor_core": tc,
+               "speedup_tc_vs_plain": plain["ms_fwd_bwd"] / tc["ms_fwd_bwd"],
+               "within_tol": plain["rel_l2_fwd_vs_fp64_oracle"] <= tol
+               and tc["rel_l2_fwd_vs_fp64_oracle"] <= tol}
         if any(s.get("tc") for s in _sm100.plan_query(dims, 0, _sm100.PLAN_TC_PRIME_AXES)["steps"]):
-            hy = run(dims, _sm100.PLAN_TC_PRIME_AXES, 10, ref)
+            hy = run(dims, x, _sm100.PLAN_TC_PRIME_AXES, ref)
             row["tc_prime_axes"] = hy
             row["speedup_hybrid_vs_plain"] = plain["ms_fwd_bwd"] / hy["ms_fwd_bwd"]
+            row["within_tol"] = row["within_tol"] and hy["rel_l2_fwd_vs_fp64_oracle"] <= tol
         res.append(row)
+    return res
+
+
+def suite_tc(args):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
     print(json.dumps({"metric": "tensor-core split-FP16 form vs plain FP32 kernels, complex64 fwd+bwd",
-                      "configs": res, "data": "synthetic, iid uniform[-1,1) seed 42"}), flush=True)
+                      "configs": tc_form(TC_SHAPES, local, per_step=True),
+                      "data": "synthetic, iid uniform[-1,1) seed 42"}), flush=True)
     return 0
+
+
+def forms(args, gpu):
+    """The three north-star forms against the plain kernels on this GPU, each
+    timing with its own clock record and its error against the oracle:
+    tensor cores (one prime-axis shape, FFT1D 2^24), batched (C4) and
+    served (C5, one offered load below saturation and one at it)."""
+    t0 = time.perf_counter()
+    out = {"tensor_core": tc_form([(65536, 61), (1 << 24,)], gpu)}
+    t1 = time.perf_counter()
+    out["batched"] = batched_form(args.count, gpu)
+    t2 = time.perf_counter()
+    out["served"] = served_form(400, gpu, loads=(0.5, 8.0))
+    out["wall_s"] = {"tensor_core": t1 - t0, "batched": t2 - t1, "served": time.perf_counter() - t2}
+    return out
 
 
 def main():

@@ -173,6 +173,13 @@ int shafft_sm100_batch_execute(shafft_sm100_batch b, void* const* src, void* con
 int shafft_sm100_batch_destroy(shafft_sm100_batch b);
 /* error flag of the last executes (call after synchronising) */
 int shafft_sm100_batch_status(shafft_sm100_batch b);
+/* Bound of each tile's wait for the previous pass of its transform: after
+ * `polls` unsuccessful polls of the pass's completion counter (about 64 ns
+ * apart) the tile sets the batch's error word and goes on, so the launch
+ * always ends and shafft_sm100_batch_status then reports
+ * SHAFFT_SM100_ECUDA.  0 restores the default (2^22 polls, far above any
+ * legitimate wait).  A small bound exists to exercise that error path. */
+int shafft_sm100_batch_set_wait_limit(shafft_sm100_batch b, unsigned polls);
 /* algorithmic HBM bytes of one execute (read + write per pass) */
 int64_t shafft_sm100_batch_bytes(shafft_sm100_batch b);
 int shafft_sm100_batch_describe(shafft_sm100_batch b, char* buf, int buflen);
@@ -271,8 +278,11 @@ int shafft_sm100_device_name(char* buf, int buflen);
  * exits.  Each call regenerates what it reads, so results do not depend on
  * earlier calls, but all calls on a device share the array: calls whose work
  * overlaps on the GPU race and corrupt each other -- issue them in order on
- * one stream.  The first call on a device looks the array's address up with
- * cudaGetSymbolAddress; make that first call before any stream capture.
+ * one stream.  The first call on each device does one-time set-up there:
+ * it looks the array's address up with cudaGetSymbolAddress, and the first
+ * call of each precision on that device raises the pass kernels' shared-
+ * memory limit (cudaFuncSetAttribute).  Make one call of each precision you
+ * use on every device before capturing a stream on it.
  * Asynchronous on `stream` (cudaStream_t, NULL = legacy default stream). */
 int shafft_sm100_bluestein_noalloc(const void* in, void* out, int64_t n, int precision,
                                    int direction, double scale, void* stream);

@@ -197,20 +197,25 @@ static void FN(stockham)(const FN(plan1d) * p, const CPLX* x, CPLX* y, CPLX* scr
     CPLX* B = bufs[cur ^ 1];
     const int64_t twstep = n / lp; /* w_{l'}^{e} = w_n^{e * n/l'} */
     const int64_t pstep = n / rad; /* w_p^{e} = w_n^{e * n/p} */
+    CPLX wp[ORACLE_DIRECT_PRIME_MAX + 4]; /* w_p^e, e < rad */
+    for (int64_t e = 0; e < rad; ++e) wp[e] = p->tw[e * pstep];
     for (int64_t s = 0; s < ns; ++s) {
       for (int64_t k = 0; k < l; ++k) {
         for (int64_t r = 0; r < rad; ++r) {
           CPLX a = A[(s + ns * r) * l + k];
-          CPLX w = p->tw[(r * k * twstep) % n];
+          CPLX w = p->tw[r * k * twstep]; /* r*k*twstep < rad*l*(n/lp) = n */
           v[r].re = a.re * w.re - a.im * w.im;
           v[r].im = a.re * w.im + a.im * w.re;
         }
         for (int64_t q = 0; q < rad; ++q) {
           REAL sr = 0, si = 0;
+          int64_t e = 0; /* (r*q) mod rad, advanced by q per r */
           for (int64_t r = 0; r < rad; ++r) {
-            CPLX w = p->tw[((r * q) % rad) * pstep];
+            CPLX w = wp[e];
             sr += v[r].re * w.re - v[r].im * w.im;
             si += v[r].re * w.im + v[r].im * w.re;
+            e += q;
+            if (e >= rad) e -= rad;
           }
           B[s * lp + k + l * q].re = sr;
           B[s * lp + k + l * q].im = si;
@@ -267,7 +272,13 @@ static int64_t FN(scratch_len)(const FN(plan1d) * p) {
 }
 
 /* Transform one axis of a row-major tensor held in work (long double or
- * double complex), in place. */
+ * double complex), in place.  Lines of a strided axis are gathered in groups
+ * of neighbouring lines (consecutive inner indices) that fill one 64-byte
+ * cache line, so each gathered cache line is used whole; every line is
+ * transformed on its own, exactly as when taken one at a time. */
+#ifndef ORACLE_LINE_GROUP
+#define ORACLE_LINE_GROUP ((int64_t)(64 / sizeof(CPLX)) > 1 ? (int64_t)(64 / sizeof(CPLX)) : 1)
+#endif
 static int FN(axis_pass)(CPLX* data, int ndim, const int64_t* dims, int axis, int sign,
                          int nthreads) {
   const int64_t n = dims[axis];
@@ -277,7 +288,12 @@ static int FN(axis_pass)(CPLX* data, int ndim, const int64_t* dims, int axis, in
   for (int a = 0; a < axis; ++a) outer *= dims[a];
   FN(plan1d)* p = FN(plan_make)(n, sign);
   if (!p) return -2;
-  const int64_t lines = outer * inner;
+  const int64_t G = inner >= ORACLE_LINE_GROUP ? ORACLE_LINE_GROUP : 1;
+  /* row pitch of the gathered lines: one element more than a power-of-two
+   * length, so that the G rows do not alias onto the same cache sets */
+  const int64_t ld = G > 1 ? n + 1 : n;
+  const int64_t per_outer = (inner + G - 1) / G;
+  const int64_t groups = outer * per_outer;
   const int64_t slen = FN(scratch_len)(p);
   int err = 0;
 #ifdef _OPENMP
@@ -285,26 +301,28 @@ static int FN(axis_pass)(CPLX* data, int ndim, const int64_t* dims, int axis, in
 #pragma omp parallel num_threads(nt)
 #endif
   {
-    CPLX* line = (CPLX*)malloc(sizeof(CPLX) * (size_t)(2 * n + slen));
-    if (!line) {
+    CPLX* lines = (CPLX*)malloc(sizeof(CPLX) * (size_t)(G * ld + slen));
+    if (!lines) {
 #ifdef _OPENMP
 #pragma omp atomic write
 #endif
       err = -2;
     } else {
-      CPLX* out = line + n;
-      CPLX* scr = out + n;
+      CPLX* scr = lines + G * ld;
 #ifdef _OPENMP
 #pragma omp for schedule(static)
 #endif
-      for (int64_t li = 0; li < lines; ++li) {
-        const int64_t o = li / inner, i = li % inner;
-        CPLX* base = data + o * n * inner + i;
-        for (int64_t k = 0; k < n; ++k) line[k] = base[k * inner];
-        FN(exec1d)(p, line, out, scr);
-        for (int64_t k = 0; k < n; ++k) base[k * inner] = out[k];
+      for (int64_t gi = 0; gi < groups; ++gi) {
+        const int64_t o = gi / per_outer, i0 = (gi % per_outer) * G;
+        const int64_t g = inner - i0 < G ? inner - i0 : G;
+        CPLX* base = data + o * n * inner + i0;
+        for (int64_t k = 0; k < n; ++k)
+          for (int64_t j = 0; j < g; ++j) lines[j * ld + k] = base[k * inner + j];
+        for (int64_t j = 0; j < g; ++j) FN(exec1d)(p, lines + j * ld, lines + j * ld, scr);
+        for (int64_t k = 0; k < n; ++k)
+          for (int64_t j = 0; j < g; ++j) base[k * inner + j] = lines[j * ld + k];
       }
-      free(line);
+      free(lines);
     }
   }
   FN(plan_free)(p);
@@ -317,6 +335,10 @@ static int FN(fftaxes)(const double* in, double* out, int ndim, const int64_t* d
   for (int a = 0; a < ndim; ++a) total *= dims[a];
   CPLX* w = (CPLX*)malloc(sizeof(CPLX) * (size_t)total);
   if (!w) return -2;
+#ifdef _OPENMP
+  const int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nt)
+#endif
   for (int64_t i = 0; i < total; ++i) {
     w[i].re = (REAL)in[2 * i];
     w[i].im = (REAL)in[2 * i + 1];
@@ -324,11 +346,15 @@ static int FN(fftaxes)(const double* in, double* out, int ndim, const int64_t* d
   int rc = 0;
   for (int i = 0; i < naxes && rc == 0; ++i)
     rc = FN(axis_pass)(w, ndim, dims, axes[i], sign, nthreads);
-  if (rc == 0)
+  if (rc == 0) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(nt)
+#endif
     for (int64_t i = 0; i < total; ++i) {
       out[2 * i] = (double)w[i].re;
       out[2 * i + 1] = (double)w[i].im;
     }
+  }
   free(w);
   return rc;
 }

@@ -62,6 +62,7 @@ def load():
                                                ctypes.c_int, ctypes.c_double, vp]
     lib.shafft_sm100_batch_destroy.argtypes = [vp]
     lib.shafft_sm100_batch_status.argtypes = [vp]
+    lib.shafft_sm100_batch_set_wait_limit.argtypes = [vp, ctypes.c_uint]
     lib.shafft_sm100_batch_bytes.argtypes = [vp]
     lib.shafft_sm100_batch_bytes.restype = ctypes.c_int64
     lib.shafft_sm100_batch_describe.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
@@ -204,6 +205,10 @@ class Batch:
 
     def status(self):
         _check(self._lib.shafft_sm100_batch_status(self.handle), "batch_status")
+
+    def set_wait_limit(self, polls: int):
+        """Bound of each tile's wait for the previous pass (0 = default)."""
+        _check(self._lib.shafft_sm100_batch_set_wait_limit(self.handle, int(polls)), "set_wait_limit")
 
     @property
     def alg_bytes(self) -> int:

@@ -81,7 +81,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1)
     k_fft_batch(const SlotDesc<typename Cx<T>::type>* slots, const int64_t* start, int nslots,
                 typename Cx<T>::type* const* src, typename Cx<T>::type* const* dst, int* done,
-                unsigned long long* ticket, int* err, int conj, double scale) {
+                unsigned long long* ticket, int* err, int conj, double scale, unsigned spin_limit) {
   using C = typename Cx<T>::type;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1)
             int v;
             asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(done + pv) : "memory");
             if (v >= need) break;
-            if (++it > kBatchSpinLimit) {
+            if (++it > spin_limit) {
               atomicExch(err, 1);
               break;
             }
@@ -217,6 +217,9 @@ struct shafft_sm100_batch_s {
   int graph_conj = -1;
   double graph_scale = 0;
   cudaStream_t graph_stream = nullptr;
+  // polls of a tile's wait for the previous pass before it gives up, sets
+  // the error word and goes on (shafft_sm100_batch_set_wait_limit)
+  unsigned wait_limit = kBatchSpinLimit;
   std::string desc;
 };
 
@@ -532,7 +535,7 @@ int batch_launch(shafft_sm100_batch_s* b, int conj, double scale, cudaStream_t s
   k_fft_batch<T><<<b->grid, kThreads, b->smem, s>>>(
       reinterpret_cast<const SlotDesc<C>*>(b->d_slots), b->d_start, b->nslots,
       reinterpret_cast<C* const*>(b->d_src), reinterpret_cast<C* const*>(b->d_dst), b->d_ctl + 4,
-      reinterpret_cast<unsigned long long*>(b->d_ctl), b->d_ctl + 2, conj, scale);
+      reinterpret_cast<unsigned long long*>(b->d_ctl), b->d_ctl + 2, conj, scale, b->wait_limit);
   BCUDA(cudaGetLastError());
   return 0;
 }
@@ -647,6 +650,17 @@ int shafft_sm100_batch_execute(shafft_sm100_batch b, void* const* src, void* con
     b->graph_stream = s;
   }
   BCUDA(cudaGraphLaunch(b->graph, s));
+  return 0;
+}
+
+int shafft_sm100_batch_set_wait_limit(shafft_sm100_batch b, unsigned polls) {
+  if (!b) return bfail(SHAFFT_SM100_EINVAL, "null batch");
+  const unsigned limit = polls ? polls : kBatchSpinLimit;
+  if (limit != b->wait_limit && b->graph) {  // the limit is a launch argument of the captured graph
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->wait_limit = limit;
   return 0;
 }
 

@@ -45,8 +45,13 @@ struct Vec2<double> {
 template <typename T>
 struct Launch {
   using C = typename Vec2<T>::type;
-  // raise the dynamic shared-memory limit of every pass kernel once
+  // raise the dynamic shared-memory limit of every pass kernel on the
+  // current device (idempotent)
   static cudaError_t init();
+  // init() once per device and element type: function attributes belong to
+  // each device's context, so a process that plans on several devices sets
+  // them on every one (thread-safe; later calls return the first result)
+  static cudaError_t init_device();
   static cudaError_t pass(const PassGeom& g, const C* in, C* out, const PassTables<C>& tb,
                           size_t smem, cudaStream_t s);
   // specialised pass for a hot length; tile width is 16 bytes x 8 (= 8*VW

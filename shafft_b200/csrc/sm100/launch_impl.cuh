@@ -5,6 +5,7 @@
 #include <stdlib.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include <cudaTypedefs.h>
 
@@ -353,6 +354,24 @@ cudaError_t Launch<T>::init() {
 #undef SHAFFT_ATTR_GENERIC
   if (e != cudaSuccess) return e;
   return fast_attr_all<T>();
+}
+
+template <typename T>
+cudaError_t Launch<T>::init_device() {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static bool done[kMaxDevices] = {};
+  static cudaError_t result[kMaxDevices] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!done[dev]) {
+    result[dev] = init();
+    done[dev] = true;
+  }
+  return result[dev];
 }
 
 template <typename T>

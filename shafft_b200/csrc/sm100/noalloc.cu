@@ -21,8 +21,10 @@
 //     concurrency on the same device) race on the array and corrupt each
 //     other; serialise them, e.g. by issuing them on one stream.
 //   * The first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress (a runtime call made once per device); make that
-//     first call before capturing a stream.
+//     cudaGetSymbolAddress (a runtime call made once per device), and the
+//     first call of each precision on a device sets the pass kernels'
+//     shared-memory limit there (cudaFuncSetAttribute, once per device and
+//     precision); make those first calls before capturing a stream.
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdint.h>
@@ -140,10 +142,7 @@ int run(const void* in, void* out, int64_t n, int direction, double scale, cudaS
   uint16_t* p2k = reinterpret_cast<uint16_t*>(base + kNoAllocSlots * 16);
   uint16_t* k2p = p2k + kNoAllocMaxM;
 
-  static std::once_flag once;
-  static cudaError_t init_err = cudaSuccess;
-  std::call_once(once, [] { init_err = K::init(); });
-  cudaError_t e = init_err;
+  cudaError_t e = K::init_device();
   if (e == cudaSuccess) e = K::gen_twiddle(twL, M, 1, M, s);
   if (e == cudaSuccess) {
     k_gen_digits<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(p2k, k2p, (int)M);

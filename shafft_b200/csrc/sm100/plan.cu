@@ -930,9 +930,7 @@ struct Launcher {
   using K = Launch<T>;
 
   static int init_once() {
-    static std::once_flag once;
-    static cudaError_t err = cudaSuccess;
-    std::call_once(once, [] { err = K::init(); });
+    const cudaError_t err = K::init_device();
     if (err != cudaSuccess) {
       g_last_cuda = (int)err;
       return set_err(SHAFFT_SM100_ECUDA, "kernel attribute setup: %s", cudaGetErrorString(err));

@@ -34,6 +34,8 @@
 // FP64 is used only where the plan builds its tables (w_L, w_N).
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+
+#include <mutex>
 #include <stdint.h>
 
 #include "kernels.cuh"
@@ -507,10 +509,12 @@ int tc_pass(const PassGeom& g, const float2* in, float2* out, const PassTables<f
             cudaStream_t s) {
   if (!tc_supported(g)) return report_error(4, "tensor-core pass: length outside 2..64");
   constexpr int kMaxDev = 64;
+  static std::mutex mu;
   static int sms[kMaxDev] = {};
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev)
     return report_error(3, "tensor-core pass: device query failed");
+  std::unique_lock<std::mutex> lk(mu);
   if (!sms[dev]) {
     int n = 0;
     if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
@@ -519,10 +523,12 @@ int tc_pass(const PassGeom& g, const float2* in, float2* out, const PassTables<f
       return report_error(3, "tensor-core pass: kernel set-up failed");
     sms[dev] = n;
   }
+  const int nsm = sms[dev];
+  lk.unlock();
   const TcLayout ly = tc_layout(g.L);
   const int64_t rows = g.ext[0] * g.ext[1] * g.ext[2] * g.ext[3];
   const int64_t ntiles = (rows + ly.RT - 1) / ly.RT;
-  const int64_t grid = ntiles < 2 * (int64_t)sms[dev] ? ntiles : 2 * (int64_t)sms[dev];
+  const int64_t grid = ntiles < 2 * (int64_t)nsm ? ntiles : 2 * (int64_t)nsm;
   if (grid < 1) return 0;
   k_fft_tc<<<(unsigned)grid, kTcThreads, ly.total, s>>>(g, in, out, tb, err);
   const cudaError_t e = cudaGetLastError();

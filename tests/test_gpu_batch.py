@@ -58,3 +58,34 @@ def test_batch_autotune_cache(tmp_path, monkeypatch):
     b.execute([d.ptr for d in src], [d.ptr for d in dst])
     for x, d in zip(xs, dst):
         assert o.rel_l2(d.download().reshape(x.shape), o.fftn(x.astype(np.complex128))) <= tol(x.size, 0)
+
+
+def test_batch_wait_timeout_sets_error_and_context_stays_usable():
+    """The bounded wait of a tile for the previous pass of its transform
+    running out: with the bound cut to one poll, tiles of the second pass
+    that are claimed while first-pass tiles are still running give up, set
+    the batch's error word and carry on, so the launch ends and
+    shafft_sm100_batch_status reports SHAFFT_SM100_ECUDA with its message.
+    Restoring the default bound, the next execute on the same context is
+    correct again.  (No trap, no unbounded wait: the kernel always returns.)"""
+    shapes = [(2048, 2048)]  # one transform, so pass-1 tiles follow pass-0 tiles at once
+    x = o.uniform_input(shapes[0], seed=9, dtype=np.complex64)
+    b = _sm100.Batch(shapes, S.C2C, autotune=False)
+    src, dst = S.DeviceBuffer(x.size), S.DeviceBuffer(x.size)
+    src.upload(x)
+    b.set_wait_limit(1)
+    messages = []
+    for _ in range(3):  # timing-dependent: one attempt is expected to suffice
+        b.execute([src.ptr], [dst.ptr], 0, 1.0, 0)
+        dst.download()  # synchronises
+        try:
+            b.status()
+        except _sm100.Sm100Error as e:
+            messages.append(str(e))
+            break
+    assert messages and "rc=3" in messages[0] and "timed out" in messages[0], messages
+    b.set_wait_limit(0)
+    b.execute([src.ptr], [dst.ptr], 0, 1.0, 0)
+    y = dst.download().reshape(x.shape)
+    b.status()
+    assert o.rel_l2(y, o.fftn(x.astype(np.complex128))) <= tol(x.size, 0)
