@@ -77,6 +77,8 @@ int MPI_Allreduce(const void* sendbuf, void* recvbuf, int count, MPI_Datatype da
                   MPI_Comm comm);
 int MPI_Allgather(const void* sendbuf, int sendcount, MPI_Datatype sendtype, void* recvbuf,
                   int recvcount, MPI_Datatype recvtype, MPI_Comm comm);
+int MPI_Gather(const void* sendbuf, int sendcount, MPI_Datatype sendtype, void* recvbuf,
+               int recvcount, MPI_Datatype recvtype, int root, MPI_Comm comm);
 int MPI_Get_processor_name(char* name, int* resultlen);
 int MPI_Error_string(int errorcode, char* string, int* resultlen);
 int MPI_Dims_create(int nnodes, int ndims, int dims[]);

@@ -124,6 +124,14 @@ int MPI_Allgather(const void* sendbuf, int sendcount, MPI_Datatype sendtype, voi
     memmove(recvbuf, sendbuf, (size_t)sendcount * (size_t)type_size(sendtype));
   return MPI_SUCCESS;
 }
+int MPI_Gather(const void* sendbuf, int sendcount, MPI_Datatype sendtype, void* recvbuf, int,
+               MPI_Datatype, int root, MPI_Comm comm) {
+  if (!known(comm)) return MPI_ERR_COMM;
+  if (root != 0) return MPI_ERR_ARG;  // the only rank is 0
+  if (sendbuf != MPI_IN_PLACE && sendbuf != recvbuf)
+    memmove(recvbuf, sendbuf, (size_t)sendcount * (size_t)type_size(sendtype));
+  return MPI_SUCCESS;
+}
 int MPI_Get_processor_name(char* name, int* resultlen) {
   if (!name || !resultlen) return MPI_ERR_ARG;
   if (gethostname(name, MPI_MAX_PROCESSOR_NAME) != 0) strcpy(name, "localhost");

@@ -28,6 +28,8 @@
 
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <new>
 #include <string>
 #include <utility>
@@ -72,6 +74,32 @@ int backend_fail(int rc, const char* what) {
     default:
       return fail(SHAFFT_ERR_BACKEND, SHAFFT_ERRSRC_HIPFFT, rc, "%s: %s", what, m);
   }
+}
+
+// Diagnostics on stderr, switched on by SHAFFT_FFT_DIAG=1 as in the
+// reference (src/cpp/fft/common/diag.hpp:17-46): one line per plan, execute
+// and normalize, tagged [SHAFFT:<module>][r<rank>][<location>].
+bool diag_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("SHAFFT_FFT_DIAG");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+void diag(const char* module, MPI_Comm comm, const char* location, const char* fmt, ...) {
+  if (!diag_enabled()) return;
+  int r = -1;
+  if (comm != MPI_COMM_NULL) MPI_Comm_rank(comm, &r);
+  char line[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(line, sizeof(line), fmt, ap);
+  va_end(ap);
+  if (r >= 0)
+    std::fprintf(stderr, "[SHAFFT:%s][r%d][%s] %s\n", module, r, location, line);
+  else
+    std::fprintf(stderr, "[SHAFFT:%s][r?][%s] %s\n", module, location, line);
 }
 
 }  // namespace
@@ -129,6 +157,10 @@ public:
     if (!data || !work) return fail(SHAFFT_ERR_NO_BUFFER);
     if (!kplan) return fail(SHAFFT_ERR_PLAN_NOT_INIT);
     const double scale = normalized ? normFactor(normExp + 1) : 1.0;
+    diag(diagModule(), comm, type == PlanType::PLAN_ND ? "fftndExecute" : "fft1dExecute",
+         "begin %s launches=%d src=%p dst=%p scale=%.17g stream=%p",
+         dir == FFTDirection::FORWARD ? "FORWARD" : "BACKWARD", shafft_sm100_plan_launches(kplan), data,
+         work, scale, (void*)stream);
     int rc = shafft_sm100_execute(kplan, data, work, dir == FFTDirection::FORWARD ? 0 : 1, scale,
                                   stream);
     if (rc) return backend_fail(rc, "execute");
@@ -139,6 +171,8 @@ public:
     std::swap(data, work);
     normExp = normalized ? 0 : normExp + 1;
     layoutState = (dir == FFTDirection::FORWARD) ? 1 : 0;
+    diag(diagModule(), comm, type == PlanType::PLAN_ND ? "fftndExecute" : "fft1dExecute",
+         "end result in data=%p pending normalize exponent=%d", data, normExp);
     return ok();
   }
 
@@ -147,6 +181,7 @@ public:
     if (!active) return ok();
     if (!data) return fail(SHAFFT_ERR_NO_BUFFER);
     const double f = normFactor(normExp);
+    diag(diagModule(), comm, "normalize", "exponent=%d factor=%.17g data=%p", normExp, f, data);
     if (f != 1.0) {
       int rc = shafft_sm100_scale(data, allocSize(), prec(), f, stream);
       if (rc) return backend_fail(rc, "normalize");
@@ -185,12 +220,23 @@ public:
     return ok();
   }
 
+  const char* diagModule() const { return type == PlanType::PLAN_ND ? "ND-sm100" : "1D-sm100"; }
+
   int plan() {
     if (!configured) return fail(SHAFFT_ERR_PLAN_NOT_INIT);
     if (planned) return fail(SHAFFT_ERR_INVALID_STATE);
     if (active) {
       int rc = createBackend();
       if (rc) return rc;
+      if (diag_enabled()) {
+        char desc[768] = "";
+        shafft_sm100_plan_describe(kplan, desc, sizeof(desc));
+        diag(diagModule(), comm, type == PlanType::PLAN_ND ? "fftndPlan" : "fft1dPlan",
+             "ndim=%d precision=%s elements=%zu launches=%d passes=%d device_bytes=%zu plan=%s",
+             ndim(), prec() ? "Z2Z(double)" : "C2C(float)", globalSize(),
+             shafft_sm100_plan_launches(kplan), shafft_sm100_plan_passes(kplan),
+             shafft_sm100_plan_device_bytes(kplan), desc);
+      }
     }
     planned = true;
     return ok();

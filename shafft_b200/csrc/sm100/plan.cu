@@ -40,6 +40,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../../include/shafft_sm100.h"
 #include "launch.h"
 #include "pass.h"
@@ -107,6 +109,17 @@ struct Step {
   int64_t planes = 0;
   size_t off_ctl = 0;  // control words (4 + planes ints) in the plan's table blob
 };
+
+// NVTX label of a step's launch (static strings: nothing is formatted on
+// the execute path)
+const char* step_label(const Step& st) {
+  if (st.kind == ST_PLANE) return "shafft_sm100 plane pass (two axes)";
+  if (st.kind == ST_COPY) return "shafft_sm100 copy";
+  if (st.kind != ST_PASS) return "shafft_sm100 bluestein element-wise step";
+  if (st.tc) return "shafft_sm100 tensor-core pass";
+  if (st.fast) return st.fast_row ? "shafft_sm100 pass (row tiles, transposing)" : "shafft_sm100 pass (column tiles)";
+  return "shafft_sm100 generic pass";
+}
 
 struct LTable {
   int L;
@@ -1041,12 +1054,16 @@ struct Launcher {
       const bool cout = last && conj;
       const double sc = last ? scale : 1.0;
       int rc;
+      // one NVTX range per launch (host-side markers for a profiler's
+      // timeline; a no-op unless a tool is attached)
+      nvtxRangePushA(step_label(st));
       if (st.kind == ST_PASS)
         rc = pass(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
       else if (st.kind == ST_PLANE)
         rc = plane(p, st, bufs[st.in_buf], bufs[st.mid_buf], bufs[st.out_buf], cin, cout, sc, s);
       else
         rc = elementwise(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
+      nvtxRangePop();
       if (rc) return rc;
     }
     return 0;

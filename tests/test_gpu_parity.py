@@ -245,3 +245,27 @@ def test_headline_sizes_vs_oracle(dims, prec):
     n = x.size
     for k, a in waves:
         assert abs(abs(y[k]) - a * n) < 0.01 * a * n
+
+
+def test_diagnostics_on_stderr():
+    """SHAFFT_FFT_DIAG=1 (the reference's switch, src/cpp/fft/common/diag.hpp:17-46)
+    prints one tagged line per plan, execute and normalize on stderr."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import shafft_b200 as S\n"
+            "p = S.FFTND(); S.check(p.init([1, 1], [32, 16]), 'init'); S.check(p.plan(), 'plan')\n"
+            "a = S.DeviceBuffer(512); b = S.DeviceBuffer(512)\n"
+            "S.check(p.set_buffers(a.ptr, b.ptr), 'set'); S.check(p.execute(S.FORWARD), 'exec')\n"
+            "S.check(p.normalize(), 'norm')\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=root,
+                       env=dict(os.environ, SHAFFT_FFT_DIAG="1"), timeout=300)
+    assert r.returncode == 0, r.stderr
+    err = r.stderr
+    assert "[SHAFFT:ND-sm100][r0][fftndPlan] ndim=2 precision=C2C(float) elements=512" in err
+    assert "[SHAFFT:ND-sm100][r0][fftndExecute] begin FORWARD" in err
+    assert "[SHAFFT:ND-sm100][r0][normalize] exponent=1" in err
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=root,
+                       env={k: v for k, v in os.environ.items() if k != "SHAFFT_FFT_DIAG"}, timeout=300)
+    assert r.returncode == 0 and "[SHAFFT:" not in r.stderr
