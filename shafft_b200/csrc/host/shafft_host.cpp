@@ -1213,6 +1213,10 @@ int shafftNDInit(void* planPtr, int ndim, int commDims[], int dimensions[], shaf
   PlanBase* b = asPlan(planPtr);
   if (b->type != shafft::PlanType::PLAN_ND) return fail(SHAFFT_ERR_INVALID_STATE);
   if (precision != SHAFFT_C2C && precision != SHAFFT_Z2Z) return fail(SHAFFT_ERR_INVALID_FFTTYPE);
+  // an output policy outside the enum is refused before anything is
+  // configured (src/c/shafftc.cpp:42-56, 91-94)
+  if (output_policy != SHAFFT_LAYOUT_REDISTRIBUTED && output_policy != SHAFFT_LAYOUT_INITIAL)
+    return fail(SHAFFT_ERR_INVALID_LAYOUT);
   return static_cast<FFTNDPlan*>(b)->configure(
       ndim, commDims, dimensions, precision == SHAFFT_Z2Z ? shafft::FFTType::Z2Z : shafft::FFTType::C2C,
       cComm,

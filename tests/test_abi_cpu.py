@@ -239,3 +239,13 @@ def test_generic_pass_tile_pitch_rule(dims, prec):
         assert s["smem"] == s["L"] * want * es, s
         seen += 1
     assert seen
+
+
+def test_nd_init_refuses_unknown_output_policy():
+    """An output policy outside {REDISTRIBUTED, INITIAL} returns
+    ERR_INVALID_LAYOUT (src/c/shafftc.cpp:42-56, 91-94; the reference's
+    tests/integration/c/test_c_api.c "shafftNDInit(invalid_policy)")."""
+    p = S.FFTND()
+    assert p.init([1, 1, 1], [16, 16, 16], output_policy=2) == 12  # SHAFFT_ERR_INVALID_LAYOUT
+    assert not p.is_configured()
+    assert p.init([1, 1, 1], [16, 16, 16], output_policy=1) == 0
