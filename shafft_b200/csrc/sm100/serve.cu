@@ -7,9 +7,9 @@
 // free instance asks a builder thread for one and lets the requests behind it
 // (up to kScanWindow) go first, so plan creation (device allocations, table
 // kernels, a synchronisation: tens of ms for large shapes) overlaps the
-// transforms instead of stalling the queue.  Memory admission stays in
-// arrival order: a request that does not fit the budget holds back the ones
-// behind it.
+// transforms instead of stalling the queue.  A request that does not fit
+// the budget lets later requests that do fit go first, up to 16 of them;
+// then it holds back the ones behind it until memory frees up.
 //   * device input/output buffers come from a stream-ordered memory pool
 //     (cudaMallocAsync / cudaFreeAsync), so freeing is ordered after the work;
 //   * plans are kept resident per shape (several instances per shape when
@@ -17,7 +17,10 @@
 //     when the budget needs their memory;
 //   * each admitted request is issued on the least recently used of S streams
 //     (H2D copy, execute, D2H copy, frees), so requests that arrive while
-//     others run overlap with them on the GPU.
+//     others run overlap with them on the GPU; requests of 64 MiB or more per
+//     buffer share one low-priority "bulk lane" stream instead, in admission
+//     order, so that large transfers do not split the host link among
+//     themselves (the first finishes in about its serial time).
 // A completion thread polls the per-request events, releases the budget and
 // the plan instance, stamps the completion time and wakes waiters.  Latency
 // is completion time minus submission time; statistics report p50 / p99.
@@ -81,6 +84,7 @@ struct Request {
   int stream = -1;
   int status = 0;
   bool done = false;
+  int passed_over = 0;  // admissions of later requests while this one did not fit
 };
 
 }  // namespace
@@ -134,6 +138,11 @@ std::string plan_key(const Request& r) {
 }
 
 constexpr size_t kScanWindow = 64;  // queued requests the dispatcher looks past a plan-blocked one
+// a request that does not fit the budget lets at most this many later
+// requests be admitted before it
+constexpr int kMaxPassOvers = 16;
+// requests with at least this many bytes per buffer use the bulk lane
+constexpr size_t kBulkLaneBytes = size_t(64) << 20;
 
 // caller holds s->mu: a free instance of r's shape (marked busy), or null
 // after asking the builder for one (unless a build of that shape runs)
@@ -273,15 +282,23 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
       }
     }
     // the first request, in arrival order, that fits the budget and has a
-    // free plan instance; a request that does not fit stops the scan
+    // free plan instance.  A request that does not fit is passed over by
+    // later ones that do, at most kMaxPassOvers times; after that it stops
+    // the scan until memory frees up for it (no starvation).
     std::shared_ptr<Request> r;
     PlanInst* inst = nullptr;
     size_t pos = 0;
     for (auto it = s->queue.begin(); it != s->queue.end() && pos < kScanWindow; ++it, ++pos) {
-      if (s->used + 2 * (*it)->bytes > s->budget) break;
+      if (s->used + 2 * (*it)->bytes > s->budget) {
+        if ((*it)->passed_over >= kMaxPassOvers) break;
+        continue;
+      }
       inst = free_instance(s, **it);
       if (inst) {
         r = *it;
+        // every earlier request that did not fit has now been passed over once
+        for (auto jt = s->queue.begin(); jt != it; ++jt)
+          if (s->used + 2 * (*jt)->bytes > s->budget) (*jt)->passed_over++;
         s->queue.erase(it);
         break;
       }
@@ -292,10 +309,17 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
     }
     const size_t need = 2 * r->bytes;
     s->used += need;
-    // least recently used stream
+    // Large requests go, in admission order, through the bulk lane (stream
+    // 0): two of them never split the host link between them, so the first
+    // finishes in about its serial time instead of both taking twice as
+    // long.  Everything else takes the least recently used of the other,
+    // higher-priority streams and so overlaps with the bulk lane.
     int si = 0;
-    for (int i = 1; i < s->nstreams; ++i)
-      if (s->stream_last[i] < s->stream_last[si]) si = i;
+    if (s->nstreams > 1 && r->bytes < kBulkLaneBytes) {
+      si = 1;
+      for (int i = 2; i < s->nstreams; ++i)
+        if (s->stream_last[i] < s->stream_last[si]) si = i;
+    }
     s->stream_last[si] = Clock::now();
     r->inst = inst;
     r->stream = si;
@@ -391,9 +415,14 @@ int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, in
     uint64_t keep = UINT64_MAX;  // keep freed blocks cached in the pool
     e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
+  int prio_low = 0, prio_high = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   for (int i = 0; e == cudaSuccess && i < streams; ++i) {
     cudaStream_t st = nullptr;
-    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    // the bulk lane (stream 0) at the lowest priority, the others at the
+    // highest: kernels of small requests get SMs first as blocks retire
+    e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking,
+                                     (i == 0 && streams > 1) ? prio_low : prio_high);
     s->streams.push_back(st);
     s->stream_last.push_back(Clock::now());
   }
