@@ -193,8 +193,7 @@ int shafft_sm100_batch_describe(shafft_sm100_batch b, char* buf, int buflen);
  * resident plans alone leave no room; a request that does not fit lets at
  * most 16 later ones that do go first), issued on the least recently used
  * of the streams (H2D, execute, D2H) and so overlap with requests already
- * running.  Requests of 64 MiB or more per buffer share stream 0, a
- * lower-priority bulk lane, in admission order.
+ * running.
  * wait() blocks until the request's output is in host_out and returns its
  * status and latency (submission to completion).  stats() reports completed
  * / failed counts, p50 / p99 / max latency, throughput and plan-instance

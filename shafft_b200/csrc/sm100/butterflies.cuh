@@ -148,6 +148,31 @@ __device__ __forceinline__ void dft16(C* v) {
   }
 }
 
+// 32 points: DFT16 of the even and the odd points, then one radix-2 stage
+// with the twiddles w32^k: X[k] = E[k] + w^k O[k], X[k+16] = E[k] - w^k O[k]
+template <int K, typename C>
+__device__ __forceinline__ void dft32_combine(C* v, const C* e, const C* o) {
+  if constexpr (K < 16) {
+    const C t = ctw<32, K>(o[K]);
+    v[K] = cadd(e[K], t);
+    v[K + 16] = csub(e[K], t);
+    dft32_combine<K + 1>(v, e, o);
+  }
+}
+
+template <typename C>
+__device__ __forceinline__ void dft32(C* v) {
+  C e[16], o[16];
+#pragma unroll
+  for (int n = 0; n < 16; ++n) {
+    e[n] = v[2 * n];
+    o[n] = v[2 * n + 1];
+  }
+  dft16(e);
+  dft16(o);
+  dft32_combine<0>(v, e, o);
+}
+
 // odd prime p: X_0 = x_0 + sum_j a_j, and for k = 1..(p-1)/2
 //   X_k     = x_0 + sum_j a_j cos(2 pi jk/p) - i sum_j b_j sin(2 pi jk/p)
 //   X_{p-k} = x_0 + sum_j a_j cos(2 pi jk/p) + i sum_j b_j sin(2 pi jk/p)
@@ -196,6 +221,8 @@ __device__ __forceinline__ void dft(C* v) {
     dft8(v);
   } else if constexpr (R == 16) {
     dft16(v);
+  } else if constexpr (R == 32) {
+    dft32(v);
   } else {
     static_assert(R == 3 || R == 5 || R == 7 || R == 11 || R == 13, "unsupported radix");
     dft_odd<R>(v);

@@ -9,7 +9,7 @@ from decimal import Decimal, getcontext
 
 getcontext().prec = 60
 PRIMES = [3, 5, 7, 11, 13]
-POW2 = [8, 16]
+POW2 = [8, 16, 32]
 
 
 def pi():

@@ -31,6 +31,17 @@ struct PassTables;
 int tc_pass(const PassGeom& g, const float2* in, float2* out, const PassTables<float2>& tb, int* err,
             cudaStream_t s);
 
+// Two axes of a stack of 512 x 512 complex64 planes in one pass, one 16-CTA
+// cluster per plane exchanging through distributed shared memory
+// (plane_cluster.cu).  plane_cluster_available() is false on a device that
+// cannot co-schedule such clusters; the planner then keeps two passes.
+bool plane_cluster_len(int precision, int64_t L);
+bool plane_cluster_available();
+size_t plane_cluster_smem();
+cudaError_t plane_cluster_pass(const float2* in, float2* out, int64_t planes, int64_t pstride_in,
+                               int64_t pstride_out, const float2* tw, int conj_in, int conj_out,
+                               double scale, cudaStream_t s);
+
 template <typename T>
 struct Vec2;
 template <>

@@ -108,12 +108,17 @@ struct Step {
   int lag = 4;
   int64_t planes = 0;
   size_t off_ctl = 0;  // control words (4 + planes ints) in the plan's table blob
+  // ST_PLANE with cluster = 1: the two axes of each L x L plane in one pass
+  // of k_fft_plane_cluster (a thread-block cluster holds the plane in
+  // distributed shared memory); in_buf -> out_buf, planes of L*L elements
+  int cluster = 0;
 };
 
 // NVTX label of a step's launch (static strings: nothing is formatted on
 // the execute path)
 const char* step_label(const Step& st) {
-  if (st.kind == ST_PLANE) return "shafft_sm100 plane pass (two axes)";
+  if (st.kind == ST_PLANE)
+    return st.cluster ? "shafft_sm100 plane pass (two axes, cluster)" : "shafft_sm100 plane pass (two axes)";
   if (st.kind == ST_COPY) return "shafft_sm100 copy";
   if (st.kind != ST_PASS) return "shafft_sm100 bluestein element-wise step";
   if (st.tc) return "shafft_sm100 tensor-core pass";
@@ -205,6 +210,7 @@ struct Planner {
     // bulk-copy column passes); 0 = ok
     off_tcerr = alloc(16);
     if (const char* e = getenv("SHAFFT_SM100_PLANE")) plane_enabled = atoi(e) != 0;
+    if (const char* e = getenv("SHAFFT_SM100_PLANE_CLUSTER")) plane_cluster_enabled = atoi(e) != 0;
     if (const char* e = getenv("SHAFFT_SM100_FLOW_LAG")) flow_lag = std::max(1, atoi(e));
     if (const char* e = getenv("SHAFFT_SM100_ROTATE")) rotate_enabled = atoi(e) != 0;
   }
@@ -395,6 +401,27 @@ struct Planner {
     return true;
   }
   int plane_enabled = 0;  // SHAFFT_SM100_PLANE=1 turns the fused plane pass on (slower so far)
+
+  // The last two axes of a stack of O L x L planes in one pass of the cluster
+  // plane kernel, in place on buf (the parity fix may turn it out of place).
+  bool plane_cluster_step(std::vector<Step>& out, int64_t O, int64_t L, int buf) {
+    if (!plane_cluster_enabled || tc_mode == 1 || !plane_cluster_len(precision, L)) return false;
+    Step st;
+    st.kind = ST_PLANE;
+    st.cluster = 1;
+    st.in_buf = st.mid_buf = st.out_buf = buf;
+    fill_radix(st.g, (int)L);
+    st.g.ext[0] = st.g.ext[1] = st.g.ext[2] = st.g.ext[3] = 1;
+    st.tabL = ltab((int)L);
+    st.smem = plane_cluster_smem();
+    st.planes = O;
+    out.push_back(st);
+    return true;
+  }
+  // SHAFFT_SM100_PLANE_CLUSTER=0 turns the cluster plane pass off; plan
+  // creation also turns it off on a device that cannot co-schedule the
+  // clusters
+  int plane_cluster_enabled = 0;
   int flow_lag = 4;       // SHAFFT_SM100_FLOW_LAG: planes between an X tile and its Y tile
 
   // The last two axes (A = rows, Lr = contiguous) as two transposing passes:
@@ -807,7 +834,11 @@ struct Planner {
       int outer = 0;
       for (int c = 0; c < b; ++c) outer += on(c);
       if (b >= 0 && !on(b)) b = -1;
-      if (b >= 0 && b == a - 1 && outer > 0) {
+      int64_t Ob = 1;
+      for (int c = 0; c < b; ++c) Ob *= dims[c];
+      if (b >= 0 && b == a - 1 && dims[b] == dims[a] && plane_cluster_step(out, Ob, dims[a], cur)) {
+        a = b - 1;
+      } else if (b >= 0 && b == a - 1 && outer > 0) {
         int64_t O = 1;
         for (int c = 0; c < b; ++c) O *= dims[c];
         if (dims[b] == dims[a] && plane_step(out, O, dims[a], cur))
@@ -841,7 +872,8 @@ struct Planner {
     for (int i = (int)out.size() - 1; i >= 0; --i) {
       Step& st = out[i];
       const bool user = (st.in_buf == BUF_SRC || st.in_buf == BUF_DST);
-      const bool inplace_pass = st.kind == ST_PASS && user && st.in_buf == st.out_buf;
+      const bool inplace_pass =
+          (st.kind == ST_PASS || (st.kind == ST_PLANE && st.cluster)) && user && st.in_buf == st.out_buf;
       const bool demod = st.kind == ST_BS_DEMOD && (st.out_buf == BUF_SRC || st.out_buf == BUF_DST);
       if (inplace_pass || demod) {
         st.out_buf = other_buf(demod ? st.out_buf : st.in_buf);
@@ -1006,6 +1038,20 @@ struct Launcher {
                  "fft pass");
   }
 
+  static int plane_cluster(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* out,
+                           bool conj_in, bool conj_out, double scale, cudaStream_t s) {
+    if constexpr (std::is_same<T, float>::value) {
+      const LTable& lt = p->ltabs[st.tabL];
+      const int64_t L = st.g.L;
+      return check(plane_cluster_pass(reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), st.planes,
+                                      L * L, L * L, reinterpret_cast<const C*>(p->d_tables + lt.off_tw),
+                                      conj_in ? 1 : 0, conj_out ? 1 : 0, scale, s),
+                   "cluster plane pass");
+    } else {
+      return set_err(SHAFFT_SM100_ENOTSUP, "cluster plane pass on a complex128 plan");
+    }
+  }
+
   static int plane(const shafft_sm100_plan_s* p, const Step& st, const void* in, void* mid, void* out,
                    bool conj_in, bool conj_out, double scale, cudaStream_t s) {
     int rc = init_once();
@@ -1059,6 +1105,8 @@ struct Launcher {
       nvtxRangePushA(step_label(st));
       if (st.kind == ST_PASS)
         rc = pass(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
+      else if (st.kind == ST_PLANE && st.cluster)
+        rc = plane_cluster(p, st, bufs[st.in_buf], bufs[st.out_buf], cin, cout, sc, s);
       else if (st.kind == ST_PLANE)
         rc = plane(p, st, bufs[st.in_buf], bufs[st.mid_buf], bufs[st.out_buf], cin, cout, sc, s);
       else
@@ -1128,7 +1176,11 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
   for (size_t i = 0; i < steps.size(); ++i) {
     const Step& st = steps[i];
     char b[768];
-    if (st.kind == ST_PLANE) {
+    if (st.kind == ST_PLANE && st.cluster) {
+      snprintf(b, sizeof(b),
+               "{\"kind\":\"plane\",\"L\":%d,\"planes\":%lld,\"cluster\":16,\"in\":\"%s\",\"out\":\"%s\",\"smem\":%zu}",
+               st.g.L, (long long)st.planes, buf_name(st.in_buf), buf_name(st.out_buf), st.smem);
+    } else if (st.kind == ST_PLANE) {
       snprintf(b, sizeof(b),
                "{\"kind\":\"plane\",\"L\":%d,\"planes\":%lld,\"lag\":%d,\"in\":\"%s\",\"mid\":\"%s\",\"out\":\"%s\",\"fast\":1}",
                st.g.L, (long long)st.planes, st.lag, buf_name(st.in_buf), buf_name(st.mid_buf),
@@ -1222,6 +1274,16 @@ int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int preci
   configure(pl, k, mask);
   int rc = pl.plan_nd(p->steps, ndim, dims);
   if (rc) return rc;
+  bool cluster_steps = false;
+  for (const Step& st : p->steps) cluster_steps |= (st.kind == ST_PLANE && st.cluster);
+  if (cluster_steps && !plane_cluster_available()) {
+    // this device cannot co-schedule the plane clusters: plan again without
+    pl = Planner(precision, flags);
+    configure(pl, k, mask);
+    pl.plane_cluster_enabled = 0;
+    rc = pl.plan_nd(p->steps, ndim, dims);
+    if (rc) return rc;
+  }
   p->off_tcerr = pl.off_tcerr;
   p->check_err = (flags & (SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES)) != 0;
   // column passes can set it only through the opt-in bulk-copy kernel
@@ -1687,7 +1749,7 @@ int shafft_sm100_plan_status(shafft_sm100_plan plan) {
                      "a pass gave up waiting (tensor-core MMA results or a bulk tensor copy)");
   }
   for (const Step& st : plan->steps) {
-    if (st.kind != ST_PLANE) continue;
+    if (st.kind != ST_PLANE || st.cluster) continue;
     int flag = 0;
     CUDA_TRY(cudaMemcpy(&flag, plan->d_tables + st.off_ctl + 2 * sizeof(int), sizeof(int),
                         cudaMemcpyDeviceToHost));

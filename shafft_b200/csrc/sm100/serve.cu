@@ -17,10 +17,7 @@
 //     when the budget needs their memory;
 //   * each admitted request is issued on the least recently used of S streams
 //     (H2D copy, execute, D2H copy, frees), so requests that arrive while
-//     others run overlap with them on the GPU; requests of 64 MiB or more per
-//     buffer share one low-priority "bulk lane" stream instead, in admission
-//     order, so that large transfers do not split the host link among
-//     themselves (the first finishes in about its serial time).
+//     others run overlap with them on the GPU.
 // A completion thread polls the per-request events, releases the budget and
 // the plan instance, stamps the completion time and wakes waiters.  Latency
 // is completion time minus submission time; statistics report p50 / p99.
@@ -141,8 +138,6 @@ constexpr size_t kScanWindow = 64;  // queued requests the dispatcher looks past
 // a request that does not fit the budget lets at most this many later
 // requests be admitted before it
 constexpr int kMaxPassOvers = 16;
-// requests with at least this many bytes per buffer use the bulk lane
-constexpr size_t kBulkLaneBytes = size_t(64) << 20;
 
 // caller holds s->mu: a free instance of r's shape (marked busy), or null
 // after asking the builder for one (unless a build of that shape runs)
@@ -309,17 +304,10 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
     }
     const size_t need = 2 * r->bytes;
     s->used += need;
-    // Large requests go, in admission order, through the bulk lane (stream
-    // 0): two of them never split the host link between them, so the first
-    // finishes in about its serial time instead of both taking twice as
-    // long.  Everything else takes the least recently used of the other,
-    // higher-priority streams and so overlaps with the bulk lane.
+    // least recently used stream
     int si = 0;
-    if (s->nstreams > 1 && r->bytes < kBulkLaneBytes) {
-      si = 1;
-      for (int i = 2; i < s->nstreams; ++i)
-        if (s->stream_last[i] < s->stream_last[si]) si = i;
-    }
+    for (int i = 1; i < s->nstreams; ++i)
+      if (s->stream_last[i] < s->stream_last[si]) si = i;
     s->stream_last[si] = Clock::now();
     r->inst = inst;
     r->stream = si;
@@ -415,14 +403,9 @@ int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, in
     uint64_t keep = UINT64_MAX;  // keep freed blocks cached in the pool
     e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
-  int prio_low = 0, prio_high = 0;
-  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   for (int i = 0; e == cudaSuccess && i < streams; ++i) {
     cudaStream_t st = nullptr;
-    // the bulk lane (stream 0) at the lowest priority, the others at the
-    // highest: kernels of small requests get SMs first as blocks retire
-    e = cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking,
-                                     (i == 0 && streams > 1) ? prio_low : prio_high);
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     s->streams.push_back(st);
     s->stream_last.push_back(Clock::now());
   }
