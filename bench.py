@@ -315,7 +315,7 @@ def kernel_name(st):
             return "k_fft_fast_tma"  # column tile fed by bulk tensor copies (when its view qualifies)
         return f"k_fft_fast<IN_ROW={st.get('in_row', 0)}>"
     if st["kind"] == "plane":
-        return "k_fft_plane_flow"
+        return "k_fft_plane_cluster" if st.get("cluster") else "k_fft_plane_flow"
     return "k_fft_pass" if st["kind"] == "pass" else f"k_bs/{st['kind']}"
 
 

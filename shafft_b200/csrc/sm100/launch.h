@@ -38,9 +38,10 @@ int tc_pass(const PassGeom& g, const float2* in, float2* out, const PassTables<f
 bool plane_cluster_len(int precision, int64_t L);
 bool plane_cluster_available();
 size_t plane_cluster_smem();
+// `err` is a device int set to 1 when a wait for the prefetch copies gives up.
 cudaError_t plane_cluster_pass(const float2* in, float2* out, int64_t planes, int64_t pstride_in,
                                int64_t pstride_out, const float2* tw, int conj_in, int conj_out,
-                               double scale, cudaStream_t s);
+                               double scale, int* err, cudaStream_t s);
 
 template <typename T>
 struct Vec2;

@@ -1045,7 +1045,8 @@ struct Launcher {
       const int64_t L = st.g.L;
       return check(plane_cluster_pass(reinterpret_cast<const C*>(in), reinterpret_cast<C*>(out), st.planes,
                                       L * L, L * L, reinterpret_cast<const C*>(p->d_tables + lt.off_tw),
-                                      conj_in ? 1 : 0, conj_out ? 1 : 0, scale, s),
+                                      conj_in ? 1 : 0, conj_out ? 1 : 0, scale,
+                                      reinterpret_cast<int*>(p->d_tables + p->off_tcerr), s),
                    "cluster plane pass");
     } else {
       return set_err(SHAFFT_SM100_ENOTSUP, "cluster plane pass on a complex128 plan");
@@ -1286,6 +1287,8 @@ int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int preci
   }
   p->off_tcerr = pl.off_tcerr;
   p->check_err = (flags & (SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES)) != 0;
+  for (const Step& st : p->steps)
+    if (st.kind == ST_PLANE && st.cluster) p->check_err = true;  // bounded prefetch waits
   // column passes can set it only through the opt-in bulk-copy kernel
   const char* tma = getenv("SHAFFT_SM100_TMA");
   if (tma && atoi(tma) != 0) {
@@ -1746,7 +1749,7 @@ int shafft_sm100_plan_status(shafft_sm100_plan plan) {
     CUDA_TRY(cudaMemcpy(&flag, plan->d_tables + plan->off_tcerr, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag)
       return set_err(SHAFFT_SM100_ECUDA,
-                     "a pass gave up waiting (tensor-core MMA results or a bulk tensor copy)");
+                     "a pass gave up waiting (tensor-core MMA results or a bulk copy)");
   }
   for (const Step& st : plan->steps) {
     if (st.kind != ST_PLANE || st.cluster) continue;

@@ -10,9 +10,14 @@
 // exchange the intermediate through distributed shared memory (DSMEM)
 // instead of HBM:
 //
+//   prefetch      the first 24 rows of the CTA's slab of its NEXT plane are
+//                 brought into a second shared buffer (96 KiB) by bulk copies
+//                 (cp.async.bulk, this GPU's memory, no multicast) on an
+//                 mbarrier while the current plane is being transformed; the
+//                 other 8 rows are loaded by the warps that need them;
 //   row phase     warp w transforms rows w and w + 16 of its CTA's slab along
-//                 the contiguous axis c (512 = 16 x 32): each lane loads the 16
-//                 points c = lane + 32 m (coalesced 256-byte rows), DFT16 in
+//                 the contiguous axis c (512 = 16 x 32): each lane takes the 16
+//                 points c = lane + 32 m (256 contiguous bytes per warp), DFT16 in
 //                 registers, twiddle w512^(lane k1), a swizzled write of the
 //                 16 x 32 block into its own slab row, DFT16 over l = 2 l2 + h
 //                 per lane pair, radix-2 between the two lanes of a pair
@@ -31,13 +36,16 @@
 //                 contiguous bytes per warp store.
 //
 // Every plane is read and written exactly once; the kernel is persistent (one
-// cluster per plane at a time, as many clusters as fit on the GPU).  The only
-// waits are the hardware cluster barriers, which every CTA of a cluster
-// reaches the same number of times (all loop over the same planes), so no
-// wait can hang.  No CTA touches another's shared memory after the last
-// barrier it shares with it.  No bulk or tensor copies are used, so no load
-// can multicast.  in == out is allowed: a plane's loads all complete before
-// the first cluster barrier of that plane and its stores all come after it.
+// cluster per plane at a time, as many clusters as fit on the GPU).  The
+// cluster barriers are reached the same number of times by every CTA of a
+// cluster (all loop over the same planes).  The prefetch wait is bounded:
+// after kPreSpinLimit polls the CTA records *err = 1, carries on (its
+// results are then wrong, never out of bounds) and, before exiting, waits --
+// bounded again -- for the copy it may still have in flight.  No CTA touches
+// another's shared memory after the last barrier it shares with it.
+// in == out is allowed: every load of a plane (prefetch included) completes
+// before the first cluster barrier of that plane, and its stores all come
+// after it.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -56,8 +64,14 @@ constexpr int kPL = 512;            // plane side
 constexpr int kCS = 16;             // CTAs per cluster (non-portable size)
 constexpr int kRows = kPL / kCS;    // 32 rows of the plane per CTA
 constexpr int kNT = 512;            // threads per CTA: 16 warps
-constexpr size_t kSmem = (size_t)kRows * kPL * sizeof(float2);  // 128 KiB
+constexpr int kPre = 24;            // rows of the next plane prefetched by bulk copies
+constexpr int kPreCopies = 6;       // bulk copies per prefetch (16 KiB each)
+constexpr size_t kSlabBytes = (size_t)kRows * kPL * sizeof(float2);  // 128 KiB
+constexpr size_t kPreBytes = (size_t)kPre * kPL * sizeof(float2);    // 96 KiB
+constexpr size_t kSmem = kSlabBytes + kPreBytes + 16;                // + mbarrier
+constexpr long long kPreSpinLimit = 1ll << 22;  // mbarrier polls before giving up
 static_assert(kNT / 32 == 16 && kRows == 32, "the thread mapping assumes 16 warps and 32 rows");
+static_assert(kPre >= 16 && kPre <= kRows && (kPreBytes / kPreCopies) % 16 == 0, "prefetch shape");
 
 __device__ __forceinline__ void cluster_arrive() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
@@ -66,66 +80,142 @@ __device__ __forceinline__ void cluster_wait() {
   asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 
+// 8-byte load from the shared memory of CTA `rank` of this cluster, at the
+// offset that `local` (a shared::cta address of this CTA) has in its own
+__device__ __forceinline__ float2 ld_dsmem(uint32_t local, int rank) {
+  uint32_t remote;
+  float2 v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(remote) : "memory");
+  return v;
+}
+
+// bounded wait for phase `parity` of the mbarrier at `bar`; false on timeout
+__device__ __forceinline__ bool pre_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done = 0;
+  for (long long i = 0; i < kPreSpinLimit && !done; ++i) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+  }
+  return done != 0;
+}
+
+// one thread: arm the mbarrier with the prefetch's bytes and copy the first
+// kPre rows of this CTA's slab of a plane into the prefetch buffer
+__device__ __forceinline__ void pre_issue(const float2* rows, uint32_t dst, uint32_t bar) {
+  constexpr uint32_t chunk = (uint32_t)(kPreBytes / kPreCopies);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((uint32_t)kPreBytes)
+               : "memory");
+#pragma unroll
+  for (int i = 0; i < kPreCopies; ++i)
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            dst + i * chunk),
+        "l"(reinterpret_cast<const char*>(rows) + (size_t)i * chunk), "r"(chunk), "r"(bar)
+        : "memory");
+}
+
+// Row phase of one row: x[m] = the row's points c = lane + 32 m.  Leaves the
+// row's 512 outputs in natural order in `row` (warp-private).
+__device__ __forceinline__ void row_fft(float2* v, float2* row, const float2* __restrict__ tw, int lane) {
+  dft16(v);  // over m: index k1
+#pragma unroll
+  for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], __ldg(tw + lane * k1));
+  // Z[l = lane][k1] at k1*32 + (l ^ 2k1): conflict-free here and in the
+  // strided gather below
+#pragma unroll
+  for (int k1 = 0; k1 < 16; ++k1) row[k1 * 32 + (lane ^ ((2 * k1) & 31))] = v[k1];
+  __syncwarp();
+  const int k1p = lane >> 1, h = lane & 1;
+#pragma unroll
+  for (int l2 = 0; l2 < 16; ++l2) v[l2] = row[k1p * 32 + ((2 * l2 + h) ^ ((2 * k1p) & 31))];
+  dft16(v);  // over l2: index k2a
+  if (h) {
+#pragma unroll
+    for (int k2a = 1; k2a < 16; ++k2a) v[k2a] = cmul(v[k2a], __ldg(tw + 16 * k2a));
+  }
+#pragma unroll
+  for (int k2a = 0; k2a < 16; ++k2a) {
+    float2 o;
+    o.x = __shfl_xor_sync(0xffffffffu, v[k2a].x, 1);
+    o.y = __shfl_xor_sync(0xffffffffu, v[k2a].y, 1);
+    v[k2a] = h ? csub(o, v[k2a]) : cadd(v[k2a], o);
+  }
+  __syncwarp();
+  // X[k1p + 16 k2a + 256 h] in natural order
+#pragma unroll
+  for (int k2a = 0; k2a < 16; ++k2a) row[k1p + 16 * k2a + 256 * h] = v[k2a];
+}
+
 __global__ void __launch_bounds__(kNT, 1)
     k_fft_plane_cluster(const float2* in, float2* out, int64_t planes, int64_t pstride_in,
                         int64_t pstride_out, const float2* __restrict__ tw, int conj_in, int conj_out,
-                        float scale) {
-  extern __shared__ __align__(128) float2 slab[];  // [kRows][kPL]
+                        float scale, int* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float2* slab = reinterpret_cast<float2*>(smem_raw);               // [kRows][kPL]
+  float2* pre = reinterpret_cast<float2*>(smem_raw + kSlabBytes);   // [kPre][kPL]
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(smem_raw + kSlabBytes + kPreBytes);
+  const uint32_t pre_s = (uint32_t)__cvta_generic_to_shared(pre);
+  const uint32_t slab_s = (uint32_t)__cvta_generic_to_shared(slab);
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   const int64_t ncl = gridDim.x / kCS;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int col = rank * kRows + lane;  // this thread's column in the column phase
+  const int64_t P0 = blockIdx.x / kCS;
+  bool failed = false;
 
-  for (int64_t P = blockIdx.x / kCS; P < planes; P += ncl) {
-    __syncthreads();  // the previous plane's column phase is done with the slab
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (P0 < planes) pre_issue(in + P0 * pstride_in + (int64_t)rank * kRows * kPL, pre_s, bar);
+  }
+  __syncthreads();
+
+  uint32_t parity = 0;
+  for (int64_t P = P0; P < planes; P += ncl, parity ^= 1) {
     // ---------------- row phase ----------------
+    // rows warp (prefetched) and warp + 16 (prefetched below kPre, else
+    // loaded from HBM now, before the wait, to overlap its latency)
     const float2* src = in + P * pstride_in + (int64_t)rank * kRows * kPL;
-#pragma unroll 1
-    for (int rr = 0; rr < 2; ++rr) {
-      float2* row = slab + (warp + 16 * rr) * kPL;
-      float2 v[16];
+    const int r1 = warp + 16;
+    float2 x[16], v[16];
+    if (r1 >= kPre) {
 #pragma unroll
-      for (int m = 0; m < 16; ++m) v[m] = __ldcs(src + (warp + 16 * rr) * kPL + lane + 32 * m);
-#pragma unroll
-      for (int m = 0; m < 16; ++m)
-        if (conj_in) v[m].y = -v[m].y;
-      dft16(v);  // over m: index k1
-#pragma unroll
-      for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], __ldg(tw + lane * k1));
-      // Z[l = lane][k1] at k1*32 + (l ^ 2k1): conflict-free here and in the
-      // strided gather below
-#pragma unroll
-      for (int k1 = 0; k1 < 16; ++k1) row[k1 * 32 + (lane ^ ((2 * k1) & 31))] = v[k1];
-      __syncwarp();
-      const int k1p = lane >> 1, h = lane & 1;
-#pragma unroll
-      for (int l2 = 0; l2 < 16; ++l2) v[l2] = row[k1p * 32 + ((2 * l2 + h) ^ ((2 * k1p) & 31))];
-      dft16(v);  // over l2: index k2a
-      if (h) {
-#pragma unroll
-        for (int k2a = 1; k2a < 16; ++k2a) v[k2a] = cmul(v[k2a], __ldg(tw + 16 * k2a));
-      }
-#pragma unroll
-      for (int k2a = 0; k2a < 16; ++k2a) {
-        float2 o;
-        o.x = __shfl_xor_sync(0xffffffffu, v[k2a].x, 1);
-        o.y = __shfl_xor_sync(0xffffffffu, v[k2a].y, 1);
-        v[k2a] = h ? csub(o, v[k2a]) : cadd(v[k2a], o);
-      }
-      __syncwarp();
-      // X[k1p + 16 k2a + 256 h] in natural order
-#pragma unroll
-      for (int k2a = 0; k2a < 16; ++k2a) row[k1p + 16 * k2a + 256 * h] = v[k2a];
+      for (int m = 0; m < 16; ++m) x[m] = __ldcs(src + r1 * kPL + lane + 32 * m);
     }
+    if (!pre_wait(bar, parity)) failed = true;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) v[m] = pre[warp * kPL + lane + 32 * m];
+    if (r1 < kPre) {
+#pragma unroll
+      for (int m = 0; m < 16; ++m) x[m] = pre[r1 * kPL + lane + 32 * m];
+    }
+    __syncthreads();  // the prefetch buffer is consumed; the slab is free
+    if (threadIdx.x == 0 && P + ncl < planes) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      pre_issue(in + (P + ncl) * pstride_in + (int64_t)rank * kRows * kPL, pre_s, bar);
+    }
+    if (conj_in) {
+#pragma unroll
+      for (int m = 0; m < 16; ++m) {
+        v[m].y = -v[m].y;
+        x[m].y = -x[m].y;
+      }
+    }
+    row_fft(v, slab + warp * kPL, tw, lane);
+    row_fft(x, slab + r1 * kPL, tw, lane);
     cl.sync();  // every slab holds its rows' transforms
     // ---------------- column phase ----------------
     float2 y[32];
 #pragma unroll
-    for (int m = 0; m < 32; ++m) {
-      const float2* rem = cl.map_shared_rank(slab, m >> 1);
-      y[m] = rem[(warp + 16 * (m & 1)) * kPL + col];
-    }
+    for (int m = 0; m < 32; ++m)
+      y[m] = ld_dsmem(slab_s + (uint32_t)(((warp + 16 * (m & 1)) * kPL + col) * sizeof(float2)), m >> 1);
     dft32(y);  // over m: index k1
     cluster_arrive();  // this CTA has read every slab it needs
 #pragma unroll
@@ -150,6 +240,13 @@ __global__ void __launch_bounds__(kNT, 1)
         __stcs(dst + (int64_t)(k1 + 32 * k2) * kPL + col, t);
       }
     }
+    __syncthreads();  // the slab is free for the next plane's rows
+  }
+  if (failed) {
+    atomicExch(err, 1);
+    // a copy may still be in flight after a wait that gave up: wait for it
+    // (bounded again) before the CTA's shared memory goes away
+    pre_wait(bar, parity ^ 1);
   }
 }
 
@@ -212,7 +309,7 @@ size_t plane_cluster_smem() { return kSmem; }
 
 cudaError_t plane_cluster_pass(const float2* in, float2* out, int64_t planes, int64_t pstride_in,
                                int64_t pstride_out, const float2* tw, int conj_in, int conj_out,
-                               double scale, cudaStream_t s) {
+                               double scale, int* err, cudaStream_t s) {
   int clusters = 0;
   if (setup(&clusters) != 1) return cudaErrorNotSupported;
   if (planes < 1) return cudaSuccess;
@@ -230,7 +327,7 @@ cudaError_t plane_cluster_pass(const float2* in, float2* out, int64_t planes, in
   cfg.dynamicSmemBytes = kSmem;
   cfg.stream = s;
   return cudaLaunchKernelEx(&cfg, k_fft_plane_cluster, in, out, planes, pstride_in, pstride_out, tw,
-                            conj_in, conj_out, (float)scale);
+                            conj_in, conj_out, (float)scale, err);
 }
 
 }  // namespace shafft_sm100
