@@ -111,16 +111,96 @@ __device__ __forceinline__ void discard_line(const void* p) {
   asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
 }
 
-// SMEM_A (column tiles only): the input tile is already in `sm` as dense
-// 128-byte rows (row p = input point p); phase A transforms it in place.
+// Base offsets of tile `tile` of a specialised pass (W = 8 * VW columns).
+struct FastTileAt {
+  int64_t w0, bin, bout, tconst;
+};
+template <int W>
+__device__ __forceinline__ FastTileAt fast_tile_at(const PassGeom& g, int64_t tile) {
+  const int64_t tw = tile % g.tiles_w;
+  int64_t rest = tile / g.tiles_w;
+  const int64_t i1 = rest % g.ext[1];
+  rest /= g.ext[1];
+  const int64_t i2 = rest % g.ext[2];
+  const int64_t i3 = rest / g.ext[2];
+  FastTileAt a;
+  a.w0 = tw * W;
+  a.bin = a.w0 * g.sin[0] + i1 * g.sin[1] + i2 * g.sin[2] + i3 * g.sin[3];
+  a.bout = a.w0 + i1 * g.sout[1] + i2 * g.sout[2] + i3 * g.sout[3];
+  a.tconst = g.tw_dim == 1 ? i1 : (g.tw_dim == 2 ? i2 : (g.tw_dim == 3 ? i3 : 0));
+  return a;
+}
+
+// Phase-A inputs of one tile: the R0 points of each of this thread's first-
+// stage butterflies, held in registers from the loads to the first stage.
+template <typename T, int L, int R0, int R1, int R2, int NT>
+struct FastRegs {
+  typename Cx<T>::type v[FastCfg<L, R0, R1, R2, NT>::NB0][R0][ChunkT<T>::VW];
+};
+
+// chunk-butterfly b of this thread: first-stage butterfly j, chunk column c
+template <int L, int R0, int NT, bool IN_ROW>
+__device__ __forceinline__ void fast_butterfly(int b, int& j, int& c) {
+  constexpr int M0 = L / R0;
+  const int id = threadIdx.x + b * NT;  // chunk-butterfly id in [0, M0*8)
+  if (IN_ROW) {
+    j = id % M0;
+    c = id / M0;
+  } else {
+    c = id & 7;
+    j = id >> 3;
+  }
+}
+
+// Phase A loads: issue every input load of tile `tile` into R.
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false>
+__device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile,
+                                          const float4* sm, int LDP, FastRegs<T, L, R0, R1, R2, NT>& R) {
+  using C = typename Cx<T>::type;
+  using Cfg = FastCfg<L, R0, R1, R2, NT>;
+  constexpr int VW = ChunkT<T>::VW;
+  constexpr int W = 8 * VW;
+  const int64_t bin = fast_tile_at<W>(g, tile).bin;
+  constexpr int M0 = L / R0;  // stride between the inputs of one butterfly
+  int bj[Cfg::NB0], bc[Cfg::NB0];
+#pragma unroll
+  for (int b = 0; b < Cfg::NB0; ++b) fast_butterfly<L, R0, NT, IN_ROW>(b, bj[b], bc[b]);
+  // issue every load first
+#pragma unroll
+  for (int b = 0; b < Cfg::NB0; ++b) {
+#pragma unroll
+    for (int r = 0; r < R0; ++r) {
+      const int n = bj[b] + r * M0;
+      if (IN_ROW) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+          R.v[b][r][e] = (LDP == LD_L2) ? ld_l2(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n)
+                                      : ld_stream(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n);
+      } else if constexpr (SMEM_A) {
+        float4 raw = sm[n * 8 + bc[b]];
+        const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) R.v[b][r][e] = ch.v[e];
+      } else {
+        const void* src = in + bin + bc[b] * VW + (int64_t)n * g.sn_in;
+        float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
+        const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) R.v[b][r][e] = ch.v[e];
+      }
+    }
+  }
+}
+
+// Phases A (first radix stage of the loaded inputs in R), B and C of tile
+// `tile`: everything after the loads.
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_,
           bool SMEM_A = false>
-__device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T>::type* in,
-                                          typename Cx<T>::type* out,
-                                          const PassTables<typename Cx<T>::type>& tb, int64_t tile,
-                                          float4* sm, TilePolicy pol = TilePolicy{0, 0, 0}) {
+__device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx<T>::type* in,
+                                            typename Cx<T>::type* out,
+                                            const PassTables<typename Cx<T>::type>& tb, int64_t tile,
+                                            float4* sm, FastRegs<T, L, R0, R1, R2, NT>& R, TilePolicy pol) {
   using C = typename Cx<T>::type;
-  const int LDP = (LDP_ == POLICY_RUNTIME) ? pol.ld : LDP_;
   const int STP = (STP_ == POLICY_RUNTIME) ? pol.st : STP_;
   const bool DISCARD = (LDP_ == POLICY_RUNTIME) ? (pol.discard != 0) : DISCARD_;
   using Cfg = FastCfg<L, R0, R1, R2, NT>;
@@ -132,61 +212,16 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
   static_assert(!(SMEM_A && IN_ROW), "shared-memory input is a column tile");
 
   const int tid = threadIdx.x;
-  const int64_t tw = tile % g.tiles_w;
-  int64_t rest = tile / g.tiles_w;
-  const int64_t i1 = rest % g.ext[1];
-  rest /= g.ext[1];
-  const int64_t i2 = rest % g.ext[2];
-  const int64_t i3 = rest / g.ext[2];
-  const int64_t w0 = tw * W;
-  const int64_t bin = w0 * g.sin[0] + i1 * g.sin[1] + i2 * g.sin[2] + i3 * g.sin[3];
-  const int64_t bout = w0 + i1 * g.sout[1] + i2 * g.sout[2] + i3 * g.sout[3];
-  const int64_t tconst = g.tw_dim == 1 ? i1 : (g.tw_dim == 2 ? i2 : (g.tw_dim == 3 ? i3 : 0));
+  const FastTileAt at = fast_tile_at<W>(g, tile);
+  const int64_t w0 = at.w0, bin = at.bin, bout = at.bout, tconst = at.tconst;
 
-  // ---------------- phase A: loads + radix-R0 stage ----------------
+  // ---------------- phase A: radix-R0 stage of the loaded inputs ----------------
   {
     constexpr int M0 = L / R0;  // stride between the inputs of one butterfly
-    C v[Cfg::NB0][R0][VW];
+    auto& v = R.v;
     int bj[Cfg::NB0], bc[Cfg::NB0];
 #pragma unroll
-    for (int b = 0; b < Cfg::NB0; ++b) {
-      const int id = tid + b * NT;  // chunk-butterfly id in [0, M0*8)
-      int j, c;
-      if (IN_ROW) {
-        j = id % M0;
-        c = id / M0;
-      } else {
-        c = id & 7;
-        j = id >> 3;
-      }
-      bj[b] = j;
-      bc[b] = c;
-    }
-    // issue every load first
-#pragma unroll
-    for (int b = 0; b < Cfg::NB0; ++b) {
-#pragma unroll
-      for (int r = 0; r < R0; ++r) {
-        const int n = bj[b] + r * M0;
-        if (IN_ROW) {
-#pragma unroll
-          for (int e = 0; e < VW; ++e)
-            v[b][r][e] = (LDP == LD_L2) ? ld_l2(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n)
-                                        : ld_stream(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n);
-        } else if constexpr (SMEM_A) {
-          float4 raw = sm[n * 8 + bc[b]];
-          const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
-#pragma unroll
-          for (int e = 0; e < VW; ++e) v[b][r][e] = ch.v[e];
-        } else {
-          const void* src = in + bin + bc[b] * VW + (int64_t)n * g.sn_in;
-          float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
-          const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
-#pragma unroll
-          for (int e = 0; e < VW; ++e) v[b][r][e] = ch.v[e];
-        }
-      }
-    }
+    for (int b = 0; b < Cfg::NB0; ++b) fast_butterfly<L, R0, NT, IN_ROW>(b, bj[b], bc[b]);
 #pragma unroll
     for (int b = 0; b < Cfg::NB0; ++b) {
 #pragma unroll
@@ -352,6 +387,20 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
       }
     }
   }
+}
+
+// SMEM_A (column tiles only): the input tile is already in `sm` as dense
+// 128-byte rows (row p = input point p); phase A transforms it in place.
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_,
+          bool SMEM_A = false>
+__device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T>::type* in,
+                                          typename Cx<T>::type* out,
+                                          const PassTables<typename Cx<T>::type>& tb, int64_t tile,
+                                          float4* sm, TilePolicy pol = TilePolicy{0, 0, 0}) {
+  const int LDP = (LDP_ == POLICY_RUNTIME) ? pol.ld : LDP_;
+  FastRegs<T, L, R0, R1, R2, NT> R;
+  fast_load<T, L, R0, R1, R2, NT, IN_ROW, SMEM_A>(g, in, tile, sm, LDP, R);
+  fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LDP_, STP_, DISCARD_, SMEM_A>(g, in, out, tb, tile, sm, R, pol);
 }
 
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW>
