@@ -260,6 +260,17 @@ int shafft_sm100_free(void* ptr);
 /* stream == NULL: synchronous copy; otherwise asynchronous on that stream. */
 int shafft_sm100_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);
 int shafft_sm100_stream_sync(void* stream);
+/* Guard bytes (debugging aid, no counterpart in the reference): with
+ * SHAFFT_SM100_CANARY=1 in the environment, shafft_sm100_malloc and the
+ * plans' own table and scratch allocations put 256 bytes of a fixed pattern
+ * before and after every block; shafft_sm100_free and plan destruction check
+ * the guards of what they release, and this call checks every live block.
+ * A changed guard byte (a kernel wrote outside its buffer) returns
+ * SHAFFT_SM100_ECUDA with the buffer and offset in the message.  Reads the
+ * guards with synchronous copies: call it with the device idle.  Returns 0
+ * when the switch is off. */
+int shafft_sm100_check_guards(void);
+
 /* Name of the current CUDA device. */
 int shafft_sm100_device_name(char* buf, int buflen);
 

@@ -76,6 +76,11 @@ def load():
     lib.shafft_sm100_server_stats.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     lib.shafft_sm100_server_reset_stats.argtypes = [vp]
     lib.shafft_sm100_server_destroy.argtypes = [vp]
+    lib.shafft_sm100_check_guards.argtypes = []
+    lib.shafft_sm100_malloc.argtypes = [ctypes.POINTER(vp), ctypes.c_size_t]
+    lib.shafft_sm100_free.argtypes = [vp]
+    lib.shafft_sm100_memcpy.argtypes = [vp, vp, ctypes.c_size_t, ctypes.c_int, vp]
+    lib.shafft_sm100_stream_sync.argtypes = [vp]
     lib.shafft_sm100_last_error_message.restype = ctypes.c_char_p
     lib.shafft_sm100_version.restype = ctypes.c_char_p
     _lib = lib

@@ -13,6 +13,13 @@ namespace shafft_sm100 {
 // shafft_sm100_last_error_message) and return `code`.
 int report_error(int code, const char* msg);
 
+// Device allocations of the library (guard.cu): plain cudaMalloc / cudaFree,
+// or, with SHAFFT_SM100_CANARY=1, blocks with guard bytes on both sides that
+// dev_free checks (a changed guard returns SHAFFT_SM100_ECUDA with a message).
+bool guard_enabled();
+cudaError_t dev_malloc(void** ptr, size_t bytes);
+int dev_free(void* ptr);
+
 // Launches of the bulk-tensor-copy column pass (k_fft_fast_tma) in this
 // process (plan.cu).
 void count_tma_launch();

@@ -1304,31 +1304,31 @@ int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int preci
   p->table_bytes = std::max<size_t>(pl.table_bytes, 256);
   p->scratch_elems = pl.scratch_elems;
   CUDA_TRY(cudaGetDevice(&p->device));
-  if (cudaMalloc(&p->d_tables, p->table_bytes) != cudaSuccess) {
+  if (dev_malloc(reinterpret_cast<void**>(&p->d_tables), p->table_bytes) != cudaSuccess) {
     cudaGetLastError();
     return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for tables failed", p->table_bytes);
   }
   if (p->scratch_elems > 0) {
     const size_t b = (size_t)p->scratch_elems * (precision ? 16 : 8);
-    if (cudaMalloc(&p->d_s0, b) != cudaSuccess || cudaMalloc(&p->d_s1, b) != cudaSuccess) {
+    if (dev_malloc(&p->d_s0, b) != cudaSuccess || dev_malloc(&p->d_s1, b) != cudaSuccess) {
       cudaGetLastError();
-      cudaFree(p->d_tables);
-      if (p->d_s0) cudaFree(p->d_s0);
+      dev_free(p->d_tables);
+      if (p->d_s0) dev_free(p->d_s0);
       return set_err(SHAFFT_SM100_EALLOC, "cudaMalloc(%zu) for scratch failed", b);
     }
   }
   if (cudaMemset(p->d_tables, 0, p->table_bytes) != cudaSuccess) {
     cudaGetLastError();
-    cudaFree(p->d_tables);
-    if (p->d_s0) cudaFree(p->d_s0);
-    if (p->d_s1) cudaFree(p->d_s1);
+    dev_free(p->d_tables);
+    if (p->d_s0) dev_free(p->d_s0);
+    if (p->d_s1) dev_free(p->d_s1);
     return set_err(SHAFFT_SM100_ECUDA, "cudaMemset of the plan tables failed");
   }
   rc = precision ? Launcher<double>::build_tables(p.get()) : Launcher<float>::build_tables(p.get());
   if (rc) {
-    cudaFree(p->d_tables);
-    if (p->d_s0) cudaFree(p->d_s0);
-    if (p->d_s1) cudaFree(p->d_s1);
+    dev_free(p->d_tables);
+    if (p->d_s0) dev_free(p->d_s0);
+    if (p->d_s1) dev_free(p->d_s1);
     return rc;
   }
   *out = p.release();
@@ -1599,12 +1599,14 @@ int shafft_sm100_plan_destroy(shafft_sm100_plan plan) {
   for (auto& g : plan->graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
-  if (plan->d_tables) cudaFree(plan->d_tables);
-  if (plan->d_s0) cudaFree(plan->d_s0);
-  if (plan->d_s1) cudaFree(plan->d_s1);
+  int rc = 0;
+  for (void* q : {static_cast<void*>(plan->d_tables), plan->d_s0, plan->d_s1}) {
+    const int r = q ? dev_free(q) : 0;  // reports changed guard bytes under SHAFFT_SM100_CANARY
+    if (!rc) rc = r;
+  }
   if (dev >= 0 && dev != plan->device) cudaSetDevice(dev);
   delete plan;
-  return 0;
+  return rc;
 }
 
 int shafft_sm100_set_stream(shafft_sm100_plan plan, void* stream) {
@@ -1787,7 +1789,7 @@ int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen) {
 int shafft_sm100_malloc(void** ptr, size_t bytes) {
   if (!ptr) return set_err(SHAFFT_SM100_EINVAL, "null pointer");
   *ptr = nullptr;
-  cudaError_t e = cudaMalloc(ptr, bytes);
+  cudaError_t e = dev_malloc(ptr, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     g_last_cuda = (int)e;
@@ -1799,8 +1801,7 @@ int shafft_sm100_malloc(void** ptr, size_t bytes) {
 
 int shafft_sm100_free(void* ptr) {
   if (!ptr) return 0;
-  CUDA_TRY(cudaFree(ptr));
-  return 0;
+  return dev_free(ptr);
 }
 
 int shafft_sm100_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
