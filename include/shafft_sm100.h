@@ -190,10 +190,11 @@ int shafft_sm100_batch_describe(shafft_sm100_batch b, char* buf, int buflen);
  * buffers -- pinned for overlap) are admitted in arrival order as soon as
  * their two device buffers fit `budget_bytes` (resident plans count against
  * the budget; idle plans are evicted oldest first, and only when the
- * resident plans alone leave no room; a request that does not fit lets at
- * most 16 later ones that do go first), issued on the least recently used
- * of the streams (H2D, execute, D2H) and so overlap with requests already
- * running.
+ * resident plans alone leave no room), issued on the least recently used
+ * of the streams (H2D, execute, D2H, in pieces of at most 8 MiB) and so
+ * overlap with requests already running.  Creation grows the device memory
+ * pool to the budget (or to what the device can spare), so request buffers
+ * are carved out of memory mapped up front.
  * wait() blocks until the request's output is in host_out and returns its
  * status and latency (submission to completion).  stats() reports completed
  * / failed counts, p50 / p99 / max latency, throughput and plan-instance

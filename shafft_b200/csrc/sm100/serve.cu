@@ -7,9 +7,9 @@
 // free instance asks a builder thread for one and lets the requests behind it
 // (up to kScanWindow) go first, so plan creation (device allocations, table
 // kernels, a synchronisation: tens of ms for large shapes) overlaps the
-// transforms instead of stalling the queue.  A request that does not fit
-// the budget lets later requests that do fit go first, up to 16 of them;
-// then it holds back the ones behind it until memory frees up.
+// transforms instead of stalling the queue.  Memory admission stays in
+// arrival order: a request that does not fit the budget holds back the ones
+// behind it.
 //   * device input/output buffers come from a stream-ordered memory pool
 //     (cudaMallocAsync / cudaFreeAsync), so freeing is ordered after the work;
 //   * plans are kept resident per shape (several instances per shape when
@@ -17,7 +17,9 @@
 //     when the budget needs their memory;
 //   * each admitted request is issued on the least recently used of S streams
 //     (H2D copy, execute, D2H copy, frees), so requests that arrive while
-//     others run overlap with them on the GPU.
+//     others run overlap with them on the GPU; the copies go in pieces of
+//     8 MiB so that a small request's copy need not wait behind a whole large
+//     transfer on a copy engine.
 // A completion thread polls the per-request events, releases the budget and
 // the plan instance, stamps the completion time and wakes waiters.  Latency
 // is completion time minus submission time; statistics report p50 / p99.
@@ -81,7 +83,6 @@ struct Request {
   int stream = -1;
   int status = 0;
   bool done = false;
-  int passed_over = 0;  // admissions of later requests while this one did not fit
 };
 
 }  // namespace
@@ -135,9 +136,6 @@ std::string plan_key(const Request& r) {
 }
 
 constexpr size_t kScanWindow = 64;  // queued requests the dispatcher looks past a plan-blocked one
-// a request that does not fit the budget lets at most this many later
-// requests be admitted before it
-constexpr int kMaxPassOvers = 16;
 
 // caller holds s->mu: a free instance of r's shape (marked busy), or null
 // after asking the builder for one (unless a build of that shape runs)
@@ -244,6 +242,21 @@ void evict_idle(shafft_sm100_server_s* s, size_t need, const std::string& keep_k
   }
 }
 
+// Host<->device copies of a request in pieces of at most kCopyChunk bytes:
+// a small request's copy on another stream can then start after one piece
+// of a large transfer already queued on the copy engine instead of after the
+// whole transfer.
+constexpr size_t kCopyChunk = size_t(8) << 20;
+cudaError_t copy_chunked(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
+  for (size_t off = 0; off < bytes; off += kCopyChunk) {
+    const size_t n = bytes - off < kCopyChunk ? bytes - off : kCopyChunk;
+    const cudaError_t e = cudaMemcpyAsync(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off,
+                                          n, kind, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 void dispatcher_loop(shafft_sm100_server_s* s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
@@ -277,23 +290,15 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
       }
     }
     // the first request, in arrival order, that fits the budget and has a
-    // free plan instance.  A request that does not fit is passed over by
-    // later ones that do, at most kMaxPassOvers times; after that it stops
-    // the scan until memory frees up for it (no starvation).
+    // free plan instance; a request that does not fit stops the scan
     std::shared_ptr<Request> r;
     PlanInst* inst = nullptr;
     size_t pos = 0;
     for (auto it = s->queue.begin(); it != s->queue.end() && pos < kScanWindow; ++it, ++pos) {
-      if (s->used + 2 * (*it)->bytes > s->budget) {
-        if ((*it)->passed_over >= kMaxPassOvers) break;
-        continue;
-      }
+      if (s->used + 2 * (*it)->bytes > s->budget) break;
       inst = free_instance(s, **it);
       if (inst) {
         r = *it;
-        // every earlier request that did not fit has now been passed over once
-        for (auto jt = s->queue.begin(); jt != it; ++jt)
-          if (s->used + 2 * (*jt)->bytes > s->budget) (*jt)->passed_over++;
         s->queue.erase(it);
         break;
       }
@@ -315,12 +320,12 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
     lk.unlock();
     cudaError_t e = cudaMallocFromPoolAsync(&r->d_in, r->bytes, s->pool, st);
     if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&r->d_out, r->bytes, s->pool, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(r->d_in, r->host_in, r->bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = copy_chunked(r->d_in, r->host_in, r->bytes, cudaMemcpyHostToDevice, st);
     int xrc = 0;
     if (e == cudaSuccess)
       xrc = shafft_sm100_execute(inst->plan, r->d_in, r->d_out, r->direction, r->scale, st);
     if (e == cudaSuccess && !xrc)
-      e = cudaMemcpyAsync(r->host_out, r->d_out, r->bytes, cudaMemcpyDeviceToHost, st);
+      e = copy_chunked(r->host_out, r->d_out, r->bytes, cudaMemcpyDeviceToHost, st);
     if (r->d_in) cudaFreeAsync(r->d_in, st);
     if (r->d_out) cudaFreeAsync(r->d_out, st);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming);
@@ -414,6 +419,21 @@ int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, in
       if (st) cudaStreamDestroy(st);
     delete s;
     return sfail(SHAFFT_SM100_ECUDA, "server set-up: %s", cudaGetErrorString(e));
+  }
+  // Grow the memory pool to the budget now (or to what the device can
+  // spare): a pool that first grows while requests run maps gigabytes of
+  // new memory on the request path, which showed as second-long stalls when
+  // the number of requests in flight first rose.  The pool keeps the memory
+  // (release threshold above), and later requests carve their buffers out
+  // of it.
+  for (size_t want = budget_bytes; want >= (size_t(1) << 30); want /= 2) {
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, want, s->pool, s->streams[0]) == cudaSuccess) {
+      cudaFreeAsync(p, s->streams[0]);
+      cudaStreamSynchronize(s->streams[0]);
+      break;
+    }
+    cudaGetLastError();
   }
   s->dispatcher = std::thread(dispatcher_loop, s);
   s->completer = std::thread(completer_loop, s);
