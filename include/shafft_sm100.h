@@ -249,6 +249,30 @@ int shafft_sm100_chirp_multiply(const void* src, void* dst, const void* factors,
                                 int64_t valid, int conj_in, int conj_out, double scale, int precision,
                                 void* stream);
 
+/* ---- Real-to-complex / complex-to-real transforms ----------------------
+ * (an extension: the reference supports C2C and Z2Z only,
+ * docs/limitations.dox:51-60).  A real tensor dims[0..ndim) whose last length
+ * L is even; its spectrum is the first L/2 + 1 frequencies of the last axis
+ * (dims[0..ndim-1), L/2 + 1 complex elements, row-major), the rest following
+ * by Hermitian symmetry -- the FFTW / cuFFT layout.  precision 0: float data
+ * and complex64 spectrum; 1: double and complex128.
+ *   execute_r2c: spectrum = scale * DFT(real)   (forward, exp(-2 pi i jk/n))
+ *   execute_c2r: real = scale * unnormalised inverse DFT of the Hermitian
+ *                spectrum, so c2r(r2c(x)) = N x for N = prod(dims)
+ * Both read their input as scratch (its contents are undefined afterwards);
+ * buffers are 16-byte aligned device memory, input and output distinct.
+ * The plan owns about 1.5x the spectrum's bytes of scratch.  Asynchronous on
+ * `stream`. */
+typedef struct shafft_sm100_rplan_s* shafft_sm100_rplan;
+int shafft_sm100_rplan_create(shafft_sm100_rplan* out, int ndim, const int64_t* dims, int precision);
+int shafft_sm100_rplan_destroy(shafft_sm100_rplan plan);
+/* complex elements of the spectrum: prod(dims[0..ndim-1)) * (L/2 + 1) */
+int64_t shafft_sm100_rplan_spectrum_elements(shafft_sm100_rplan plan);
+int shafft_sm100_execute_r2c(shafft_sm100_rplan plan, void* real_in, void* spec_out, double scale,
+                             void* stream);
+int shafft_sm100_execute_c2r(shafft_sm100_rplan plan, void* spec_in, void* real_out, double scale,
+                             void* stream);
+
 /* Device memory and stream helpers, so that callers above this ABI need no
  * CUDA runtime of their own (they replace the reference's allocBufferT /
  * freeBufferT / copyToBufferT / copyFromBufferT,

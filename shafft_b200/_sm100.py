@@ -76,6 +76,12 @@ def load():
     lib.shafft_sm100_server_stats.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     lib.shafft_sm100_server_reset_stats.argtypes = [vp]
     lib.shafft_sm100_server_destroy.argtypes = [vp]
+    lib.shafft_sm100_rplan_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, i64p, ctypes.c_int]
+    lib.shafft_sm100_rplan_destroy.argtypes = [vp]
+    lib.shafft_sm100_rplan_spectrum_elements.argtypes = [vp]
+    lib.shafft_sm100_rplan_spectrum_elements.restype = ctypes.c_int64
+    lib.shafft_sm100_execute_r2c.argtypes = [vp, vp, vp, ctypes.c_double, vp]
+    lib.shafft_sm100_execute_c2r.argtypes = [vp, vp, vp, ctypes.c_double, vp]
     lib.shafft_sm100_check_guards.argtypes = []
     lib.shafft_sm100_malloc.argtypes = [ctypes.POINTER(vp), ctypes.c_size_t]
     lib.shafft_sm100_free.argtypes = [vp]
@@ -165,6 +171,47 @@ class Plan:
     def destroy(self):
         if self.handle:
             self._lib.shafft_sm100_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class RPlan:
+    """Real-to-complex / complex-to-real plan (shafft_sm100_rplan_*): real
+    tensor `dims` (last length even) <-> its half spectrum (..., L/2 + 1)."""
+
+    def __init__(self, dims, precision=0):
+        lib = load()
+        self._lib = lib
+        self.dims = tuple(int(x) for x in dims)
+        self.precision = int(precision)
+        h = ctypes.c_void_p()
+        d = (ctypes.c_int64 * len(self.dims))(*self.dims)
+        _check(lib.shafft_sm100_rplan_create(ctypes.byref(h), len(self.dims), d, self.precision),
+               "rplan_create")
+        self.handle = h
+
+    @property
+    def spectrum_elements(self) -> int:
+        return int(self._lib.shafft_sm100_rplan_spectrum_elements(self.handle))
+
+    def r2c(self, real_ptr: int, spec_ptr: int, scale: float = 1.0, stream: int = 0):
+        _check(self._lib.shafft_sm100_execute_r2c(self.handle, ctypes.c_void_p(real_ptr),
+                                                  ctypes.c_void_p(spec_ptr), float(scale),
+                                                  ctypes.c_void_p(stream)), "execute_r2c")
+
+    def c2r(self, spec_ptr: int, real_ptr: int, scale: float = 1.0, stream: int = 0):
+        _check(self._lib.shafft_sm100_execute_c2r(self.handle, ctypes.c_void_p(spec_ptr),
+                                                  ctypes.c_void_p(real_ptr), float(scale),
+                                                  ctypes.c_void_p(stream)), "execute_c2r")
+
+    def destroy(self):
+        if self.handle:
+            self._lib.shafft_sm100_rplan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -249,3 +249,17 @@ def test_nd_init_refuses_unknown_output_policy():
     assert p.init([1, 1, 1], [16, 16, 16], output_policy=2) == 12  # SHAFFT_ERR_INVALID_LAYOUT
     assert not p.is_configured()
     assert p.init([1, 1, 1], [16, 16, 16], output_policy=1) == 0
+
+
+def test_real_transform_plan_refuses_odd_last_axis():
+    """shafft_sm100_rplan_create checks its shape before touching a device:
+    an odd last length is refused with SHAFFT_SM100_ENOTSUP."""
+    import ctypes
+    from shafft_b200 import _sm100
+    lib = _sm100.load()
+    h = ctypes.c_void_p()
+    dims = (ctypes.c_int64 * 2)(3, 5)
+    assert lib.shafft_sm100_rplan_create(ctypes.byref(h), 2, dims, 0) == 4
+    assert b"even" in lib.shafft_sm100_last_error_message()
+    dims = (ctypes.c_int64 * 1)(0)
+    assert lib.shafft_sm100_rplan_create(ctypes.byref(h), 1, dims, 0) == 1
