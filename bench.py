@@ -457,7 +457,7 @@ def ours(args):
         "clocks": clocks.summary(),
     }
     if world == 1 and not args.no_forms and dims == DIMS:
-        out["configs"] = configs_rows(args, local)
+        out["configs"] = configs_rows(args, local) + [r2c_row(local)]
         out["forms"] = forms(args, local)
     if dist is not None:
         dist.barrier()
@@ -928,12 +928,48 @@ def configs_rows(args, gpu, rows=CONFIG_ROWS):
     return res
 
 
+def r2c_row(gpu, dims=(256, 256, 256)):
+    """Real-to-complex then complex-to-real (fused 1/N) of a float tensor:
+    fwd+bwd time, spectrum error against the oracle, round-trip error."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as o
+    from shafft_b200 import _sm100
+    stream = torch.cuda.current_stream()
+    n = math.prod(dims)
+    H = dims[-1] // 2
+    rng = np.random.Generator(np.random.MT19937(42))
+    x = rng.uniform(-1, 1, size=dims).astype(np.float32)
+    plan = _sm100.RPlan(dims, 0)
+    xin = torch.from_numpy(x.copy()).cuda()
+    spec = torch.empty(plan.spectrum_elements, dtype=torch.complex64, device="cuda")
+    y = torch.empty(n, dtype=torch.float32, device="cuda")
+    plan.r2c(xin.data_ptr(), spec.data_ptr(), 1.0, stream.cuda_stream)
+    ref = o.fftn(x.astype(np.complex128))[..., :H + 1]
+    err = o.rel_l2(spec.cpu().numpy().reshape(ref.shape), ref)
+    del ref
+    plan.c2r(spec.data_ptr(), y.data_ptr(), 1.0 / n, stream.cuda_stream)
+    rt = o.rel_l2(y.cpu().numpy().reshape(dims), x)
+
+    def fwd_bwd():
+        plan.r2c(y.data_ptr(), spec.data_ptr(), 1.0, stream.cuda_stream)
+        plan.c2r(spec.data_ptr(), y.data_ptr(), 1.0 / n, stream.cuda_stream)
+    ms, reps, clk = timed_region(fwd_bwd, stream, gpu)
+    plan.destroy()
+    tol = 1e-6 * math.log2(n)
+    return {"dims": list(dims), "precision": "f32 -> c64 (R2C / C2R)", "ms_fwd_bwd": ms, "reps": reps,
+            "compulsory_gbs": 2 * (4 * n + 8 * n // dims[-1] * (H + 1)) / (ms / 1e3) / 1e9,
+            "rel_l2_fwd_vs_oracle": err, "roundtrip_rel_l2": rt, "tol": tol,
+            "within_tol": err <= tol and rt <= tol, "clocks": clk}
+
+
 def suite_configs(args):
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     print(json.dumps({"metric": "other configurations (512^3 aside): fwd+bwd time and error",
-                      "configs": configs_rows(args, local)}), flush=True)
+                      "configs": configs_rows(args, local) + [r2c_row(local)]}), flush=True)
     return 0
 
 
