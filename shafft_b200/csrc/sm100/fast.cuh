@@ -153,9 +153,12 @@ __device__ __forceinline__ void fast_butterfly(int b, int& j, int& c) {
 }
 
 // Phase A loads: issue every input load of tile `tile` into R.
+// Column tiles with PassGeom::bs_mode & BS_LOAD_MOD read the Bluestein
+// modulation of x on the fly (see pass.h); `chirp` is its table.
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false>
 __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile,
-                                          const float4* sm, int LDP, FastRegs<T, L, R0, R1, R2, NT>& R) {
+                                          const float4* sm, int LDP, FastRegs<T, L, R0, R1, R2, NT>& R,
+                                          const typename Cx<T>::type* chirp = nullptr) {
   using C = typename Cx<T>::type;
   using Cfg = FastCfg<L, R0, R1, R2, NT>;
   constexpr int VW = ChunkT<T>::VW;
@@ -181,6 +184,18 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
         for (int e = 0; e < VW; ++e) R.v[b][r][e] = ch.v[e];
+      } else if (g.bs_mode & BS_LOAD_MOD) {
+        // element-wise: a row of x has bs_L points (any alignment)
+        const int64_t mask = ((int64_t)1 << g.bs_logM) - 1;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+          const int64_t vo = bin + bc[b] * VW + e + (int64_t)n * g.sn_in;
+          const int64_t p = vo & mask;
+          C x = p < g.bs_L ? ld_stream(in + (vo >> g.bs_logM) * g.bs_L + p) : C{0, 0};
+          const C w = p < g.bs_L ? ld_tw(chirp + p) : C{0, 0};
+          if (g.conj_in) x.y = -x.y;
+          R.v[b][r][e] = cmul(x, w);
+        }
       } else {
         const void* src = in + bin + bc[b] * VW + (int64_t)n * g.sn_in;
         float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
@@ -230,7 +245,7 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
 #pragma unroll
         for (int r = 0; r < R0; ++r) {
           x[r] = v[b][r][e];
-          if (g.conj_in) x[r].y = -x[r].y;
+          if (g.conj_in && !(g.bs_mode & BS_LOAD_MOD)) x[r].y = -x[r].y;  // the fused load conjugates
         }
         dft<R0>(x);
         if (bj[b] != 0) {
@@ -375,10 +390,30 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
             }
             y = cmul(y, twc[e]);
           }
+          if (g.bs_mode & (BS_STORE_MULH | BS_STORE_DEMOD)) {
+            const int64_t vo = bout + c * VW + e + (int64_t)k * g.sk_out;
+            const int64_t p = vo & (((int64_t)1 << g.bs_logM) - 1);
+            if (g.bs_mode & BS_STORE_MULH) {
+              y = cmul(y, ld_tw(tb.bs_H + p));
+              y.y = -y.y;
+            } else {
+              if (p < g.bs_L) {
+                C a = y;
+                a.y = -a.y;
+                C r = cmul(ld_tw(tb.bs_chirp + p), a);
+                r.x *= scale;
+                r.y *= scale;
+                if (g.conj_out) r.y = -r.y;
+                out[(vo >> g.bs_logM) * g.bs_L + p] = r;
+              }
+              continue;
+            }
+          }
           if (g.scale != 1.0) y = cscale(y, scale);
           if (g.conj_out) y.y = -y.y;
           ch.v[e] = y;
         }
+        if (g.bs_mode & BS_STORE_DEMOD) continue;  // stored element-wise above
         float4* dstp = reinterpret_cast<float4*>(out + bout + c * VW + (int64_t)k * g.sk_out);
         if (STP == ST_STREAM)
           st_chunk(dstp, *reinterpret_cast<float4*>(&ch));
@@ -399,7 +434,7 @@ __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T
                                           float4* sm, TilePolicy pol = TilePolicy{0, 0, 0}) {
   const int LDP = (LDP_ == POLICY_RUNTIME) ? pol.ld : LDP_;
   FastRegs<T, L, R0, R1, R2, NT> R;
-  fast_load<T, L, R0, R1, R2, NT, IN_ROW, SMEM_A>(g, in, tile, sm, LDP, R);
+  fast_load<T, L, R0, R1, R2, NT, IN_ROW, SMEM_A>(g, in, tile, sm, LDP, R, tb.bs_chirp);
   fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LDP_, STP_, DISCARD_, SMEM_A>(g, in, out, tb, tile, sm, R, pol);
 }
 

@@ -107,7 +107,20 @@ struct PassGeom {
   int64_t tw_mask;
   int conj_in, conj_out;
   double scale;
+  // Bluestein steps fused into a specialised pass (bits; 0 = none):
+  //   BS_LOAD_MOD    load x (rows of bs_L, stride 1) into the virtual rows of
+  //                  2^bs_logM points: conj_in(x[p]) * chirp[p] for p < bs_L,
+  //                  0 beyond (replaces the modulate step before the pass);
+  //   BS_STORE_MULH  store conj(y * H[p]) (the spectrum multiply after it);
+  //   BS_STORE_DEMOD store conj_out(chirp[p] * conj(y) * scale) to rows of
+  //                  bs_L points, p < bs_L only (the demodulate after it);
+  // p is the point's position in its virtual row of 2^bs_logM points.
+  int bs_mode;
+  int bs_logM;
+  int64_t bs_L;
 };
+
+enum BsMode : int { BS_LOAD_MOD = 1, BS_STORE_MULH = 2, BS_STORE_DEMOD = 4 };
 
 // Shared-memory row pitch (elements) of a generic-pass tile [L][pitch] whose
 // rows hold W columns.  Column-input passes put the W columns of a row on
@@ -132,6 +145,8 @@ struct PassTables {
   const C* tw_hi;          // w_N^{(m >> shift) << shift}
   const C* tw_lo;          // w_N^{m & mask}
   const void* tcB;         // tensor-core passes: split DFT matrix in shared-memory layout
+  const C* bs_chirp;       // Bluestein fused into the pass (PassGeom::bs_mode)
+  const C* bs_H;
 };
 
 }  // namespace shafft_sm100

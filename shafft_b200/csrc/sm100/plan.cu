@@ -815,7 +815,80 @@ struct Planner {
   // axes to transform (bit a = axis a); the others are batch axes
   uint64_t axes_mask = ~0ull;
 
+  // SHAFFT_SM100_BS_FUSE=0 keeps Bluestein's element-wise steps as launches
+  // of their own (for comparisons); by default they are fused into the
+  // neighbouring specialised passes
+  static bool bs_fuse_enabled() {
+    const char* e = getenv("SHAFFT_SM100_BS_FUSE");
+    return !(e && atoi(e) == 0);
+  }
+
+  // Fold Bluestein's element-wise steps into the specialised passes next to
+  // them (rows of x with unit stride only): modulate into the loads of the
+  // first pass of the forward convolution FFT when that pass reads column
+  // tiles, the spectrum multiply into the stores of that FFT's last pass,
+  // the demodulate (with the normalisation and output conjugation) into the
+  // stores of the inverse FFT's last pass.  The same operations in the same
+  // order as the unfused steps (results agree to rounding: the compiler may
+  // contract them into fused multiply-adds differently in the two kernels).
+  // Complex64 only: measured on B200, FFT1D 1,000,003 fwd+bwd went 0.141 ->
+  // 0.123 ms fused, while complex128 went 0.296 -> 0.306 ms (its first
+  // convolution pass is 16 points long, where the element-wise loads cost
+  // more than the modulate kernel they replace).
+  void fuse_bluestein(std::vector<Step>& out) {
+    if (!bs_fuse_enabled() || precision != 0) return;
+    auto fast_pass = [](const Step& st) { return st.kind == ST_PASS && st.fast && !st.tc; };
+    auto logm = [](int64_t M) {
+      int l = 0;
+      while ((int64_t(1) << l) < M) ++l;
+      return l;
+    };
+    for (size_t i = 0; i < out.size(); ++i) {
+      Step& st = out[i];
+      if (st.kind == ST_BS_MOD && st.bsI == 1 && i + 1 < out.size()) {
+        Step& nx = out[i + 1];
+        if (fast_pass(nx) && !nx.fast_row && nx.in_buf == st.out_buf && !nx.g.bs_mode) {
+          nx.in_buf = st.in_buf;
+          nx.g.bs_mode |= BS_LOAD_MOD;
+          nx.g.bs_logM = logm(st.bsM);
+          nx.g.bs_L = st.bsL;
+          nx.tabB = st.tabB;
+          out.erase(out.begin() + i);
+          --i;
+        }
+      } else if (st.kind == ST_BS_MULH && i > 0) {
+        Step& pv = out[i - 1];
+        if (fast_pass(pv) && pv.out_buf == st.in_buf && st.in_buf == st.out_buf &&
+            !(pv.g.bs_mode & (BS_STORE_MULH | BS_STORE_DEMOD)) && (pv.tabB < 0 || pv.tabB == st.tabB)) {
+          pv.g.bs_mode |= BS_STORE_MULH;
+          pv.g.bs_logM = logm(st.bsM);
+          pv.tabB = st.tabB;
+          out.erase(out.begin() + i);
+          --i;
+        }
+      } else if (st.kind == ST_BS_DEMOD && st.bsI == 1 && i > 0) {
+        Step& pv = out[i - 1];
+        if (fast_pass(pv) && pv.out_buf == st.in_buf &&
+            !(pv.g.bs_mode & (BS_STORE_MULH | BS_STORE_DEMOD)) && (pv.tabB < 0 || pv.tabB == st.tabB)) {
+          pv.out_buf = st.out_buf;
+          pv.g.bs_mode |= BS_STORE_DEMOD;
+          pv.g.bs_logM = logm(st.bsM);
+          pv.g.bs_L = st.bsL;
+          pv.tabB = st.tabB;
+          out.erase(out.begin() + i);
+          --i;
+        }
+      }
+    }
+  }
+
   int plan_nd(std::vector<Step>& out, int ndim, const int64_t* dims) {
+    const int rc = plan_nd_steps(out, ndim, dims);
+    if (!rc) fuse_bluestein(out);
+    return rc;
+  }
+
+  int plan_nd_steps(std::vector<Step>& out, int ndim, const int64_t* dims) {
     out.clear();
     auto on = [&](int a) { return dims[a] > 1 && ((axes_mask >> a) & 1ull); };
     const bool all_axes = (ndim >= 64) || ((~axes_mask) & ((1ull << ndim) - 1)) == 0;
@@ -990,6 +1063,11 @@ struct Launcher {
     tb.p2k = reinterpret_cast<const uint16_t*>(p->d_tables + lt.off_p2k);
     tb.k2p = reinterpret_cast<const uint16_t*>(p->d_tables + lt.off_k2p);
     if (lt.tc_bytes) tb.tcB = p->d_tables + lt.off_tcB;
+    if (st.g.bs_mode && st.tabB >= 0) {
+      const BTable& bt = p->btabs[st.tabB];
+      tb.bs_chirp = reinterpret_cast<const C*>(p->d_tables + bt.off_chirp);
+      tb.bs_H = reinterpret_cast<const C*>(p->d_tables + bt.off_H);
+    }
     if (st.tabN >= 0) {
       const NTable& nt = p->ntabs[st.tabN];
       tb.tw_hi = reinterpret_cast<const C*>(p->d_tables + nt.off_hi);
@@ -1192,11 +1270,11 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
       snprintf(b, sizeof(b),
                "{\"kind\":\"pass\",\"L\":%d,\"radices\":[%s],\"W\":%d,\"in\":\"%s\",\"out\":\"%s\","
                "\"in_row\":%d,\"out_row\":%d,\"tiles\":%lld,\"smem\":%zu,\"twiddle\":%d,"
-               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d,\"tc\":%d}",
+               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d,\"tc\":%d,\"bs\":%d}",
                st.g.L, rad.c_str(), st.g.W, buf_name(st.in_buf), buf_name(st.out_buf), st.g.in_row,
                st.g.out_row, (long long)st.g.ntiles, st.smem, st.g.tw_mode, (long long)st.g.ext[0],
                (long long)st.g.ext[1], (long long)st.g.ext[2], (long long)st.g.ext[3],
-               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast, st.tc);
+               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast, st.tc, st.g.bs_mode);
     } else {
       const char* k = st.kind == ST_BS_MOD    ? "bluestein_modulate"
                       : st.kind == ST_BS_MULH ? "bluestein_multiply"
@@ -1718,6 +1796,14 @@ int64_t shafft_sm100_step_bytes(shafft_sm100_plan plan, int step) {
   if (st.kind == ST_PASS) {
     int64_t n = (int64_t)st.g.L;
     for (int d = 0; d < 4; ++d) n *= st.g.ext[d];
+    if (st.g.bs_mode & (BS_LOAD_MOD | BS_STORE_DEMOD)) {
+      // the x side of a fused modulate / demodulate touches bs_L of every
+      // 2^bs_logM points
+      const int64_t xb = (n >> st.g.bs_logM) * st.g.bs_L;
+      const int64_t rd = (st.g.bs_mode & BS_LOAD_MOD) ? xb : n;
+      const int64_t wr = (st.g.bs_mode & BS_STORE_DEMOD) ? xb : n;
+      return (rd + wr) * es;
+    }
     return 2 * n * es;
   }
   if (st.kind == ST_BS_MOD) return (st.total / st.bsM * st.bsL + st.total) * es;
