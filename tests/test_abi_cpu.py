@@ -155,7 +155,15 @@ def test_planner_pass_lists():
     assert all(s["fast"] for s in q["steps"])
     q = _sm100.plan_query([256, 256, 256], 1)
     assert [s["kind"] for s in q["steps"]] == ["pass"] * 3
+    # Bluestein, M = 2^21 = 128^3: complex64 fuses the modulate into the first
+    # pass's loads and the multiply / demodulate into the stores of the last
+    # passes of the two convolution FFTs (bs bits 1, 2, 4); complex128 keeps
+    # the element-wise steps
     q = _sm100.plan_query([1000003], 0)
+    assert [s["kind"] for s in q["steps"]] == ["pass"] * 6
+    assert [s["bs"] for s in q["steps"]] == [1, 0, 2, 0, 0, 4]
+    assert [s["in"] for s in q["steps"]][0] == "src" and q["steps"][-1]["out"] == "dst"
+    q = _sm100.plan_query([1000003], 1)
     kinds = [s["kind"] for s in q["steps"]]
     assert kinds[0] == "bluestein_modulate" and kinds[-1] == "bluestein_demodulate"
     assert q["steps"][0]["M"] == 1 << 21
