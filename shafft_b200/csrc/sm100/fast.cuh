@@ -153,9 +153,12 @@ __device__ __forceinline__ void fast_butterfly(int b, int& j, int& c) {
 }
 
 // Phase A loads: issue every input load of tile `tile` into R.
-// Column tiles with PassGeom::bs_mode & BS_LOAD_MOD read the Bluestein
-// modulation of x on the fly (see pass.h); `chirp` is its table.
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false>
+// BS instantiations only (Bluestein steps): column tiles with
+// PassGeom::bs_mode & BS_LOAD_MOD read the Bluestein modulation of x on the
+// fly (see pass.h); `chirp` is its table.  The plain instantiations carry
+// none of this code: the runtime test alone slowed the 512-point pass by a
+// quarter.
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false, bool BS = false>
 __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile,
                                           const float4* sm, int LDP, FastRegs<T, L, R0, R1, R2, NT>& R,
                                           const typename Cx<T>::type* chirp = nullptr) {
@@ -184,7 +187,7 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
         for (int e = 0; e < VW; ++e) R.v[b][r][e] = ch.v[e];
-      } else if (g.bs_mode & BS_LOAD_MOD) {
+      } else if (BS && (g.bs_mode & BS_LOAD_MOD)) {
         // element-wise: a row of x has bs_L points (any alignment)
         const int64_t mask = ((int64_t)1 << g.bs_logM) - 1;
 #pragma unroll
@@ -210,7 +213,7 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
 // Phases A (first radix stage of the loaded inputs in R), B and C of tile
 // `tile`: everything after the loads.
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_,
-          bool SMEM_A = false>
+          bool SMEM_A = false, bool BS = false>
 __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx<T>::type* in,
                                             typename Cx<T>::type* out,
                                             const PassTables<typename Cx<T>::type>& tb, int64_t tile,
@@ -245,7 +248,7 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
 #pragma unroll
         for (int r = 0; r < R0; ++r) {
           x[r] = v[b][r][e];
-          if (g.conj_in && !(g.bs_mode & BS_LOAD_MOD)) x[r].y = -x[r].y;  // the fused load conjugates
+          if (g.conj_in && !(BS && (g.bs_mode & BS_LOAD_MOD))) x[r].y = -x[r].y;  // the fused load conjugates
         }
         dft<R0>(x);
         if (bj[b] != 0) {
@@ -390,7 +393,7 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
             }
             y = cmul(y, twc[e]);
           }
-          if (g.bs_mode & (BS_STORE_MULH | BS_STORE_DEMOD)) {
+          if (BS && (g.bs_mode & (BS_STORE_MULH | BS_STORE_DEMOD))) {
             const int64_t vo = bout + c * VW + e + (int64_t)k * g.sk_out;
             const int64_t p = vo & (((int64_t)1 << g.bs_logM) - 1);
             if (g.bs_mode & BS_STORE_MULH) {
@@ -413,7 +416,7 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
           if (g.conj_out) y.y = -y.y;
           ch.v[e] = y;
         }
-        if (g.bs_mode & BS_STORE_DEMOD) continue;  // stored element-wise above
+        if (BS && (g.bs_mode & BS_STORE_DEMOD)) continue;  // stored element-wise above
         float4* dstp = reinterpret_cast<float4*>(out + bout + c * VW + (int64_t)k * g.sk_out);
         if (STP == ST_STREAM)
           st_chunk(dstp, *reinterpret_cast<float4*>(&ch));
@@ -427,23 +430,24 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
 // SMEM_A (column tiles only): the input tile is already in `sm` as dense
 // 128-byte rows (row p = input point p); phase A transforms it in place.
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_,
-          bool SMEM_A = false>
+          bool SMEM_A = false, bool BS = false>
 __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T>::type* in,
                                           typename Cx<T>::type* out,
                                           const PassTables<typename Cx<T>::type>& tb, int64_t tile,
                                           float4* sm, TilePolicy pol = TilePolicy{0, 0, 0}) {
   const int LDP = (LDP_ == POLICY_RUNTIME) ? pol.ld : LDP_;
   FastRegs<T, L, R0, R1, R2, NT> R;
-  fast_load<T, L, R0, R1, R2, NT, IN_ROW, SMEM_A>(g, in, tile, sm, LDP, R, tb.bs_chirp);
-  fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LDP_, STP_, DISCARD_, SMEM_A>(g, in, out, tb, tile, sm, R, pol);
+  fast_load<T, L, R0, R1, R2, NT, IN_ROW, SMEM_A, BS>(g, in, tile, sm, LDP, R, tb.bs_chirp);
+  fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LDP_, STP_, DISCARD_, SMEM_A, BS>(g, in, out, tb, tile, sm, R, pol);
 }
 
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW>
+// BS: the instantiation with the fused Bluestein loads and stores
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool BS = false>
 __global__ void __launch_bounds__(NT)
     k_fft_fast(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
                typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  fast_tile<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false>(
+  fast_tile<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false, false, BS>(
       g, in, out, tb, blockIdx.x, reinterpret_cast<float4*>(smem_raw));
 }
 

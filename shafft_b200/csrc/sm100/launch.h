@@ -7,6 +7,8 @@
 
 #include "pass.h"
 
+struct shafft_sm100_plan_s;
+
 namespace shafft_sm100 {
 
 // Record `msg` as this thread's last error of the library (returned by
@@ -23,6 +25,13 @@ int dev_free(void* ptr);
 // Launches of the bulk-tensor-copy column pass (k_fft_fast_tma) in this
 // process (plan.cu).
 void count_tma_launch();
+
+// True when executes of `plan` may run at the same time on different
+// streams (plan.cu): it has no scratch buffers and no step with per-launch
+// control words, so every launch reads only the plan's tables and the
+// caller's buffers (its error word is only ever set, by a bounded wait that
+// gave up).
+bool plan_shareable(const shafft_sm100_plan_s* plan);
 
 // Tensor-core (tcgen05, split FP16) pass for complex64: one DFT stage of
 // length 2..64 over every row of the geometry g (tc.cu).  `err` is a device

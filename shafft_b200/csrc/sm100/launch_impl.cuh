@@ -210,6 +210,37 @@ static cudaError_t launch_flow(KernelT kernel, int threads, size_t smem, const P
   return cudaGetLastError();
 }
 
+// The specialised pass with the fused Bluestein loads and stores
+// (k_fft_fast<..., BS = true>): instantiated for complex64 only, the one
+// precision the planner fuses; complex128 reports cudaErrorNotSupported.
+template <typename T, int L, int A, int B, int C_, int NT>
+struct FastBs {
+  static cudaError_t attr() { return cudaSuccess; }
+  static cudaError_t launch(bool, unsigned, const PassGeom&, const typename Vec2<T>::type*,
+                            typename Vec2<T>::type*, const PassTables<typename Vec2<T>::type>&, cudaStream_t) {
+    return cudaErrorNotSupported;
+  }
+};
+template <int L, int A, int B, int C_, int NT>
+struct FastBs<float, L, A, B, C_, NT> {
+  static cudaError_t attr() {
+    cudaError_t e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, true, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, false, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+    return e;
+  }
+  static cudaError_t launch(bool in_row, unsigned grid, const PassGeom& g, const float2* in, float2* out,
+                            const PassTables<float2>& tb, cudaStream_t s) {
+    if (in_row)
+      k_fft_fast<float, L, A, B, C_, NT, true, true><<<grid, NT, L * 128, s>>>(g, in, out, tb);
+    else
+      k_fft_fast<float, L, A, B, C_, NT, false, true><<<grid, NT, L * 128, s>>>(g, in, out, tb);
+    return cudaGetLastError();
+  }
+};
+
 #define SHAFFT_DEFINE_PRECISION(TYPE, FASTLIST, PLANELIST)                                       \
   template <>                                                                                    \
   cudaError_t fast_attr_all<TYPE>() {                                                            \
@@ -244,7 +275,7 @@ static cudaError_t launch_flow(KernelT kernel, int threads, size_t smem, const P
   cudaError_t Launch<TYPE>::fast(const PassGeom& g, bool in_row, const C* in, C* out,            \
                                  const PassTables<C>& tb, int* err, cudaStream_t s) {            \
     const unsigned grid = (unsigned)g.ntiles;                                                    \
-    if (!in_row && err && tma_enabled()) {                                                       \
+    if (!in_row && err && !g.bs_mode && tma_enabled()) {                                         \
       CUtensorMap map;                                                                           \
       TmaDims d;                                                                                 \
       switch (g.L) {                                                                             \
@@ -276,7 +307,8 @@ static cudaError_t fast_attr_all();
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);               \
   if (e == cudaSuccess)                                                                           \
     e = cudaFuncSetAttribute(k_fft_fast<TYPE_, L, A, B, C_, NT, false>,                           \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);               \
+  if (e == cudaSuccess) e = FastBs<TYPE_, L, A, B, C_, NT>::attr();
 #define SHAFFT_ATTR_PLANE(L, A, B, C_, NT)                                                        \
   if (e == cudaSuccess)                                                                           \
     e = cudaFuncSetAttribute(k_fft_plane_flow<TYPE_, L, A, B, C_, NT>,                            \
@@ -310,6 +342,7 @@ static cudaError_t fast_attr_all();
     return NT;
 #define SHAFFT_CASE_FAST(L_, A, B, C_, NT)                                                       \
   case L_:                                                                                       \
+    if (g.bs_mode) return FastBs<TYPE_, L_, A, B, C_, NT>::launch(in_row, grid, g, in, out, tb, s); \
     if (in_row)                                                                                  \
       k_fft_fast<TYPE_, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);      \
     else                                                                                         \

@@ -1598,6 +1598,13 @@ static int misaligned() {
 namespace shafft_sm100 {
 static std::atomic<int64_t> g_tma_launches{0};
 void count_tma_launch() { g_tma_launches.fetch_add(1, std::memory_order_relaxed); }
+
+bool plan_shareable(const shafft_sm100_plan_s* plan) {
+  if (!plan || plan->scratch_elems > 0) return false;
+  for (const Step& st : plan->steps)
+    if (st.kind == ST_PLANE) return false;  // zeroes and counts its control words every launch
+  return true;
+}
 }  // namespace shafft_sm100
 
 extern "C" {

@@ -12,9 +12,10 @@
 // behind it.
 //   * device input/output buffers come from a stream-ordered memory pool
 //     (cudaMallocAsync / cudaFreeAsync), so freeing is ordered after the work;
-//   * plans are kept resident per shape (several instances per shape when
-//     requests of one shape overlap); idle instances are evicted oldest-first
-//     when the budget needs their memory;
+//   * plans are kept resident per shape; requests of one shape that overlap
+//     share its instance when the plan has no scratch or control state
+//     (plan_shareable), and get instances of their own otherwise; idle
+//     instances are evicted oldest-first when the budget needs their memory;
 //   * each admitted request is issued on the least recently used of S streams
 //     (H2D copy, execute, D2H copy, frees), so requests that arrive while
 //     others run overlap with them on the GPU; the copies go in pieces of
@@ -61,7 +62,8 @@ using Clock = std::chrono::steady_clock;
 
 struct PlanInst {
   shafft_sm100_plan plan = nullptr;
-  bool busy = false;
+  int users = 0;        // requests in flight on this instance
+  bool shared = false;  // plan_shareable: any number of users at once
   size_t bytes = 0;
   Clock::time_point last_used;
 };
@@ -137,15 +139,16 @@ std::string plan_key(const Request& r) {
 
 constexpr size_t kScanWindow = 64;  // queued requests the dispatcher looks past a plan-blocked one
 
-// caller holds s->mu: a free instance of r's shape (marked busy), or null
-// after asking the builder for one (unless a build of that shape runs)
+// caller holds s->mu: an instance of r's shape that can take another user
+// (its user count raised), or null after asking the builder for one (unless
+// a build of that shape runs)
 PlanInst* free_instance(shafft_sm100_server_s* s, const Request& r) {
   const std::string key = plan_key(r);
   auto it = s->plans.find(key);
   if (it != s->plans.end())
     for (auto& p : it->second)
-      if (!p->busy) {
-        p->busy = true;
+      if (p->users == 0 || p->shared) {
+        p->users++;
         p->last_used = Clock::now();
         return p.get();
       }
@@ -196,6 +199,7 @@ void builder_loop(shafft_sm100_server_s* s) {
     } else {
       auto inst = std::make_unique<PlanInst>();
       inst->plan = pl;
+      inst->shared = plan_shareable(pl);
       inst->bytes = shafft_sm100_plan_device_bytes(pl);
       inst->last_used = Clock::now();
       s->plan_bytes += inst->bytes;
@@ -222,7 +226,7 @@ void evict_idle(shafft_sm100_server_s* s, size_t need, const std::string& keep_k
     for (auto& kv : s->plans) {
       if (kv.first == keep_key) continue;  // the waiting request's own shape
       for (auto& p : kv.second)
-        if (!p->busy && (!victim || p->last_used < victim->last_used)) {
+        if (p->users == 0 && (!victim || p->last_used < victim->last_used)) {
           victim = p.get();
           vkey = kv.first;
         }
@@ -337,7 +341,7 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
       r->done = true;
       r->t_done = Clock::now();
       s->used -= need;
-      inst->busy = false;
+      inst->users--;
       s->failed++;
       s->cv_done.notify_all();
       continue;
@@ -374,7 +378,7 @@ void completer_loop(shafft_sm100_server_s* s) {
       cudaEventDestroy(r->ev);
       r->ev = nullptr;
       s->used -= 2 * r->bytes;
-      r->inst->busy = false;
+      r->inst->users--;
       r->inst->last_used = Clock::now();
       r->done = true;
       s->inflight.erase(s->inflight.begin() + i);
