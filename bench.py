@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-forms", action="store_true",
                     help="leave the configs / forms objects out of the default line")
-    ap.add_argument("--suite", default="headline", choices=["headline", "batched", "serve", "configs", "tc"],
+    ap.add_argument("--suite", default="headline", choices=["headline", "batched", "serve", "configs", "tc", "exchange"],
                     help="headline (default, the contract line) or one of the side workloads")
     ap.add_argument("--count", type=int, default=4096, help="transforms of the batched suite")
     return ap.parse_args()
@@ -1058,6 +1058,64 @@ def suite_tc(args):
     return 0
 
 
+def exchange_rows(gpu, cases=((256, 2), (128, 4), (64, 8))):
+    """The local device steps before a slab exchange of 512^3 complex64 on
+    P ranks (one rank's block of 512/P x 512 x 512, axes 1 and 2, then the
+    pack along axis 1 into P per-peer blocks): the plain subplan followed by
+    the separate pack kernel against the subplan with the pack fused into its
+    last pass's stores.  Both outputs are compared."""
+    import torch
+
+    from shafft_b200.slab import CudaOps
+    ops = CudaOps(0)
+    stream = torch.cuda.current_stream()
+    rows = []
+    for m, parts in cases:
+        dims = [m, 512, 512]
+        n = math.prod(dims)
+        g = torch.Generator(device="cuda").manual_seed(7)
+        x0 = (torch.rand(2 * n, device="cuda", generator=g) * 2 - 1).view(torch.complex64)
+        a, b, c = torch.empty_like(x0), torch.empty_like(x0), torch.empty_like(x0)
+        h0 = ops.plan(dims, [1, 2])
+        h1, fused = ops.plan_mapped(dims, [1, 2], None, (m, 512, 512, parts))
+
+        def separate():
+            ops.execute(h0, a, b, 0)
+            ops.pack(b, c, m, 512, 512, parts)
+
+        def fused_step():
+            ops.execute(h1, a, b, 0)
+        a.copy_(x0)
+        separate()
+        ref = c.clone()
+        a.copy_(x0)
+        fused_step()
+        err = float((torch.linalg.vector_norm(b - ref) / torch.linalg.vector_norm(ref)).item())
+        del ref
+        ms_sep, reps_sep, clk_sep = timed_region(separate, stream, gpu)
+        ms_fused, reps_fused, clk_fused = timed_region(fused_step, stream, gpu)
+        ops.destroy(h0)
+        ops.destroy(h1)
+        rows.append({"ranks": parts, "local_block": dims, "fused_bits": fused,
+                     "ms_subplan_plus_pack": ms_sep, "ms_fused": ms_fused, "speedup": ms_sep / ms_fused,
+                     "rel_l2_fused_vs_separate": err, "tol": 1e-6 * math.log2(n),
+                     "clocks": {"separate": clk_sep, "fused": clk_fused}})
+        del x0, a, b, c
+        torch.cuda.empty_cache()
+    return rows
+
+
+def suite_exchange(args):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    print(json.dumps({"metric": "device steps before a slab exchange (512^3 complex64): subplan + pack "
+                                "vs the pack fused into the subplan's stores",
+                      "unit": "ms", "configs": exchange_rows(local),
+                      "data": "synthetic, iid uniform[-1,1)"}), flush=True)
+    return 0
+
+
 def forms(args, gpu):
     """The three north-star forms against the plain kernels on this GPU, each
     timing with its own clock record and its error against the oracle:
@@ -1085,6 +1143,8 @@ def main():
         return suite_configs(args)
     if args.suite == "tc":
         return suite_tc(args)
+    if args.suite == "exchange":
+        return suite_exchange(args)
     return ours(args)
 
 

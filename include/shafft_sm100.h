@@ -86,6 +86,30 @@ int shafft_sm100_plan_create_nd_ex(shafft_sm100_plan* out, int ndim, const int64
 int shafft_sm100_plan_create_axes(shafft_sm100_plan* out, int ndim, const int64_t* dims,
                                   int precision, int flags, int naxes, const int* axes);
 
+/* Like shafft_sm100_plan_create_axes, with a slab / pencil exchange's block
+ * packing fused into the plan: load_map / store_map = {outer, n, inner,
+ * parts} (NULL or parts = 0: none) say that the input is read from / the
+ * output is written to the per-peer block layout of the row-major array
+ * [outer][n][inner] (outer * n * inner = the plan's elements): block p,
+ * holding indices [start_p, start_p + len_p) of the n axis, is the contiguous
+ * segment [outer][len_p][inner] at offset outer * start_p * inner, with the
+ * block partition of shafft_sm100_pack_blocks.  A map is fused when n,
+ * inner and parts are powers of two (even blocks) and the plan's first step
+ * (load) or last step (store) is an out-of-place specialised pass whose
+ * accesses stay inside runs of `inner` elements;
+ * *fused returns bit 0 = load map fused, bit 1 = store map fused (a one-step
+ * plan takes only the store map).  A map that is not fused is not applied:
+ * the caller packs or unpacks with shafft_sm100_pack_blocks /
+ * shafft_sm100_unpack_blocks instead.  Replaces the separate pack / unpack
+ * of the reference's slab exchange (src/cpp/slab_nd.cpp:23-56, 596-654). */
+int shafft_sm100_plan_create_axes_mapped(shafft_sm100_plan* out, int ndim, const int64_t* dims,
+                                         int precision, int flags, int naxes, const int* axes,
+                                         const int64_t* load_map, const int64_t* store_map, int* fused);
+/* The steps such a plan would have, as shafft_sm100_plan_describe JSON with
+ * "fused" added (planning only: no device work, callable without a GPU). */
+int shafft_sm100_plan_query_mapped(int ndim, const int64_t* dims, int precision, int naxes, const int* axes,
+                                   const int64_t* load_map, const int64_t* store_map, char* buf, int buflen);
+
 /* Plan a 1-D C2C transform of length n (equivalent to the 1-D ND plan). */
 int shafft_sm100_plan_create_1d(shafft_sm100_plan* out, int64_t n, int precision);
 

@@ -105,6 +105,20 @@ PLAN_TC_PRIME_AXES = 2
 PLAN_MEASURE = 4
 
 
+def plan_query_mapped(dims, axes, precision=0, load_map=None, store_map=None) -> dict:
+    """Planning-only description of an axis-subset plan with exchange block
+    maps (shafft_sm100_plan_query_mapped); "fused" = bit 0 load, bit 1 store."""
+    lib = load()
+    d = (ctypes.c_int64 * len(dims))(*[int(x) for x in dims])
+    a = (ctypes.c_int * len(axes))(*[int(x) for x in axes])
+    lm = None if load_map is None else (ctypes.c_int64 * 4)(*load_map)
+    sm = None if store_map is None else (ctypes.c_int64 * 4)(*store_map)
+    buf = ctypes.create_string_buffer(1 << 16)
+    _check(lib.shafft_sm100_plan_query_mapped(len(dims), d, int(precision), len(axes), a, lm, sm, buf, len(buf)),
+           "plan_query_mapped")
+    return json.loads(buf.value.decode())
+
+
 def plan_query(dims, precision=0, flags=0) -> dict:
     """Host-only planner query (no GPU needed)."""
     lib = load()

@@ -152,13 +152,27 @@ __device__ __forceinline__ void fast_butterfly(int b, int& j, int& c) {
   }
 }
 
+// Block-layout index of natural index v (PassGeom::map_*, pass.h).
+__device__ __forceinline__ int64_t map_block(const PassGeom& g, int64_t v) {
+  const int64_t i = v & (((int64_t)1 << g.map_log_inner) - 1);
+  const int64_t t = v >> g.map_log_inner;
+  const int64_t k = t & (((int64_t)1 << g.map_log_n) - 1);
+  const int64_t o = t >> g.map_log_n;
+  const int64_t p = k >> g.map_log_q, kk = k & (((int64_t)1 << g.map_log_q) - 1);
+  return ((((p * g.map_outer + o) << g.map_log_q) + kk) << g.map_log_inner) + i;
+}
+
+// Extended instantiations of the specialised pass (template argument EXT).
+enum FastExtKind : int { EXT_BS = 1, EXT_MAP = 2 };
+
 // Phase A loads: issue every input load of tile `tile` into R.
-// BS instantiations only (Bluestein steps): column tiles with
-// PassGeom::bs_mode & BS_LOAD_MOD read the Bluestein modulation of x on the
-// fly (see pass.h); `chirp` is its table.  The plain instantiations carry
-// none of this code: the runtime test alone slowed the 512-point pass by a
-// quarter.
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false, bool BS = false>
+// EXT instantiations only: column tiles with PassGeom::bs_mode & BS_LOAD_MOD
+// read the Bluestein modulation of x on the fly (see pass.h; `chirp` is its
+// table), and map_mode & MAP_LOAD reads the input from an exchange's block
+// layout.  The plain instantiations carry none of this code: a runtime test
+// of bs_mode alone slowed the 512-point pass by a quarter; the two kinds are
+// separate instantiations so that each keeps its own register budget.
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false, int EXT = 0>
 __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile,
                                           const float4* sm, int LDP, FastRegs<T, L, R0, R1, R2, NT>& R,
                                           const typename Cx<T>::type* chirp = nullptr) {
@@ -179,15 +193,18 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
       const int n = bj[b] + r * M0;
       if (IN_ROW) {
 #pragma unroll
-        for (int e = 0; e < VW; ++e)
-          R.v[b][r][e] = (LDP == LD_L2) ? ld_l2(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n)
-                                      : ld_stream(in + bin + (int64_t)(bc[b] * VW + e) * g.sin[0] + n);
+        for (int e = 0; e < VW; ++e) {
+          int64_t row = bin + (int64_t)(bc[b] * VW + e) * g.sin[0];
+          // a row of L points lies in one run of 2^map_log_inner (the planner checks)
+          if ((EXT & EXT_MAP) && (g.map_mode & MAP_LOAD)) row = map_block(g, row);
+          R.v[b][r][e] = (LDP == LD_L2) ? ld_l2(in + row + n) : ld_stream(in + row + n);
+        }
       } else if constexpr (SMEM_A) {
         float4 raw = sm[n * 8 + bc[b]];
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
         for (int e = 0; e < VW; ++e) R.v[b][r][e] = ch.v[e];
-      } else if (BS && (g.bs_mode & BS_LOAD_MOD)) {
+      } else if ((EXT & EXT_BS) && (g.bs_mode & BS_LOAD_MOD)) {
         // element-wise: a row of x has bs_L points (any alignment)
         const int64_t mask = ((int64_t)1 << g.bs_logM) - 1;
 #pragma unroll
@@ -200,7 +217,9 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
           R.v[b][r][e] = cmul(x, w);
         }
       } else {
-        const void* src = in + bin + bc[b] * VW + (int64_t)n * g.sn_in;
+        int64_t off = bin + bc[b] * VW + (int64_t)n * g.sn_in;
+        if ((EXT & EXT_MAP) && (g.map_mode & MAP_LOAD)) off = map_block(g, off);  // a chunk lies in one run
+        const void* src = in + off;
         float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
@@ -213,7 +232,7 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
 // Phases A (first radix stage of the loaded inputs in R), B and C of tile
 // `tile`: everything after the loads.
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_,
-          bool SMEM_A = false, bool BS = false>
+          bool SMEM_A = false, int EXT = 0>
 __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx<T>::type* in,
                                             typename Cx<T>::type* out,
                                             const PassTables<typename Cx<T>::type>& tb, int64_t tile,
@@ -248,7 +267,7 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
 #pragma unroll
         for (int r = 0; r < R0; ++r) {
           x[r] = v[b][r][e];
-          if (g.conj_in && !(BS && (g.bs_mode & BS_LOAD_MOD))) x[r].y = -x[r].y;  // the fused load conjugates
+          if (g.conj_in && !((EXT & EXT_BS) && (g.bs_mode & BS_LOAD_MOD))) x[r].y = -x[r].y;  // the fused load conjugates
         }
         dft<R0>(x);
         if (bj[b] != 0) {
@@ -393,7 +412,7 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
             }
             y = cmul(y, twc[e]);
           }
-          if (BS && (g.bs_mode & (BS_STORE_MULH | BS_STORE_DEMOD))) {
+          if ((EXT & EXT_BS) && (g.bs_mode & (BS_STORE_MULH | BS_STORE_DEMOD))) {
             const int64_t vo = bout + c * VW + e + (int64_t)k * g.sk_out;
             const int64_t p = vo & (((int64_t)1 << g.bs_logM) - 1);
             if (g.bs_mode & BS_STORE_MULH) {
@@ -416,8 +435,10 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
           if (g.conj_out) y.y = -y.y;
           ch.v[e] = y;
         }
-        if (BS && (g.bs_mode & BS_STORE_DEMOD)) continue;  // stored element-wise above
-        float4* dstp = reinterpret_cast<float4*>(out + bout + c * VW + (int64_t)k * g.sk_out);
+        if ((EXT & EXT_BS) && (g.bs_mode & BS_STORE_DEMOD)) continue;  // stored element-wise above
+        int64_t off = bout + c * VW + (int64_t)k * g.sk_out;
+        if ((EXT & EXT_MAP) && (g.map_mode & MAP_STORE)) off = map_block(g, off);  // a chunk lies in one run
+        float4* dstp = reinterpret_cast<float4*>(out + off);
         if (STP == ST_STREAM)
           st_chunk(dstp, *reinterpret_cast<float4*>(&ch));
         else
@@ -430,24 +451,25 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
 // SMEM_A (column tiles only): the input tile is already in `sm` as dense
 // 128-byte rows (row p = input point p); phase A transforms it in place.
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int LDP_, int STP_, bool DISCARD_,
-          bool SMEM_A = false, bool BS = false>
+          bool SMEM_A = false, int EXT = 0>
 __device__ __forceinline__ void fast_tile(const PassGeom& g, const typename Cx<T>::type* in,
                                           typename Cx<T>::type* out,
                                           const PassTables<typename Cx<T>::type>& tb, int64_t tile,
                                           float4* sm, TilePolicy pol = TilePolicy{0, 0, 0}) {
   const int LDP = (LDP_ == POLICY_RUNTIME) ? pol.ld : LDP_;
   FastRegs<T, L, R0, R1, R2, NT> R;
-  fast_load<T, L, R0, R1, R2, NT, IN_ROW, SMEM_A, BS>(g, in, tile, sm, LDP, R, tb.bs_chirp);
-  fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LDP_, STP_, DISCARD_, SMEM_A, BS>(g, in, out, tb, tile, sm, R, pol);
+  fast_load<T, L, R0, R1, R2, NT, IN_ROW, SMEM_A, EXT>(g, in, tile, sm, LDP, R, tb.bs_chirp);
+  fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LDP_, STP_, DISCARD_, SMEM_A, EXT>(g, in, out, tb, tile, sm, R, pol);
 }
 
-// BS: the instantiation with the fused Bluestein loads and stores
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool BS = false>
+// EXT: the plain pass (0), or the instantiation with the fused Bluestein
+// loads and stores (EXT_BS) or with an exchange block map (EXT_MAP)
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int EXT = 0>
 __global__ void __launch_bounds__(NT)
     k_fft_fast(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
                typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  fast_tile<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false, false, BS>(
+  fast_tile<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false, false, EXT>(
       g, in, out, tb, blockIdx.x, reinterpret_cast<float4*>(smem_raw));
 }
 

@@ -210,34 +210,49 @@ static cudaError_t launch_flow(KernelT kernel, int threads, size_t smem, const P
   return cudaGetLastError();
 }
 
-// The specialised pass with the fused Bluestein loads and stores
-// (k_fft_fast<..., BS = true>): instantiated for complex64 only, the one
-// precision the planner fuses; complex128 reports cudaErrorNotSupported.
+// The extended instantiations of the specialised pass, k_fft_fast<..., EXT>:
+// EXT_BS with the fused Bluestein loads and stores (complex64 plans only;
+// PassGeom::bs_mode) and EXT_MAP with an exchange block map (map_mode).
+// Plain passes launch the instantiation without either.
+template <typename T, int L, int A, int B, int C_, int NT, int X>
+static cudaError_t fast_ext_attr() {
+  cudaError_t e = cudaFuncSetAttribute(k_fft_fast<T, L, A, B, C_, NT, true, X>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_fft_fast<T, L, A, B, C_, NT, false, X>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+  return e;
+}
+template <typename T, int L, int A, int B, int C_, int NT, int X>
+static cudaError_t fast_ext_launch(bool in_row, unsigned grid, const PassGeom& g, const typename Vec2<T>::type* in,
+                                   typename Vec2<T>::type* out, const PassTables<typename Vec2<T>::type>& tb,
+                                   cudaStream_t s) {
+  if (in_row)
+    k_fft_fast<T, L, A, B, C_, NT, true, X><<<grid, NT, L * 128, s>>>(g, in, out, tb);
+  else
+    k_fft_fast<T, L, A, B, C_, NT, false, X><<<grid, NT, L * 128, s>>>(g, in, out, tb);
+  return cudaGetLastError();
+}
 template <typename T, int L, int A, int B, int C_, int NT>
-struct FastBs {
-  static cudaError_t attr() { return cudaSuccess; }
-  static cudaError_t launch(bool, unsigned, const PassGeom&, const typename Vec2<T>::type*,
-                            typename Vec2<T>::type*, const PassTables<typename Vec2<T>::type>&, cudaStream_t) {
-    return cudaErrorNotSupported;
+struct FastExt {
+  static cudaError_t attr() { return fast_ext_attr<T, L, A, B, C_, NT, EXT_MAP>(); }
+  static cudaError_t launch(bool in_row, unsigned grid, const PassGeom& g, const typename Vec2<T>::type* in,
+                            typename Vec2<T>::type* out, const PassTables<typename Vec2<T>::type>& tb,
+                            cudaStream_t s) {
+    if (g.bs_mode) return cudaErrorNotSupported;
+    return fast_ext_launch<T, L, A, B, C_, NT, EXT_MAP>(in_row, grid, g, in, out, tb, s);
   }
 };
 template <int L, int A, int B, int C_, int NT>
-struct FastBs<float, L, A, B, C_, NT> {
+struct FastExt<float, L, A, B, C_, NT> {
   static cudaError_t attr() {
-    cudaError_t e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, true, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_fft_fast<float, L, A, B, C_, NT, false, true>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
-    return e;
+    const cudaError_t e = fast_ext_attr<float, L, A, B, C_, NT, EXT_BS>();
+    return e == cudaSuccess ? fast_ext_attr<float, L, A, B, C_, NT, EXT_MAP>() : e;
   }
   static cudaError_t launch(bool in_row, unsigned grid, const PassGeom& g, const float2* in, float2* out,
                             const PassTables<float2>& tb, cudaStream_t s) {
-    if (in_row)
-      k_fft_fast<float, L, A, B, C_, NT, true, true><<<grid, NT, L * 128, s>>>(g, in, out, tb);
-    else
-      k_fft_fast<float, L, A, B, C_, NT, false, true><<<grid, NT, L * 128, s>>>(g, in, out, tb);
-    return cudaGetLastError();
+    if (g.bs_mode) return fast_ext_launch<float, L, A, B, C_, NT, EXT_BS>(in_row, grid, g, in, out, tb, s);
+    return fast_ext_launch<float, L, A, B, C_, NT, EXT_MAP>(in_row, grid, g, in, out, tb, s);
   }
 };
 
@@ -275,7 +290,7 @@ struct FastBs<float, L, A, B, C_, NT> {
   cudaError_t Launch<TYPE>::fast(const PassGeom& g, bool in_row, const C* in, C* out,            \
                                  const PassTables<C>& tb, int* err, cudaStream_t s) {            \
     const unsigned grid = (unsigned)g.ntiles;                                                    \
-    if (!in_row && err && !g.bs_mode && tma_enabled()) {                                         \
+    if (!in_row && err && !g.bs_mode && !g.map_mode && tma_enabled()) {                          \
       CUtensorMap map;                                                                           \
       TmaDims d;                                                                                 \
       switch (g.L) {                                                                             \
@@ -308,7 +323,7 @@ static cudaError_t fast_attr_all();
   if (e == cudaSuccess)                                                                           \
     e = cudaFuncSetAttribute(k_fft_fast<TYPE_, L, A, B, C_, NT, false>,                           \
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);               \
-  if (e == cudaSuccess) e = FastBs<TYPE_, L, A, B, C_, NT>::attr();
+  if (e == cudaSuccess) e = FastExt<TYPE_, L, A, B, C_, NT>::attr();
 #define SHAFFT_ATTR_PLANE(L, A, B, C_, NT)                                                        \
   if (e == cudaSuccess)                                                                           \
     e = cudaFuncSetAttribute(k_fft_plane_flow<TYPE_, L, A, B, C_, NT>,                            \
@@ -342,7 +357,7 @@ static cudaError_t fast_attr_all();
     return NT;
 #define SHAFFT_CASE_FAST(L_, A, B, C_, NT)                                                       \
   case L_:                                                                                       \
-    if (g.bs_mode) return FastBs<TYPE_, L_, A, B, C_, NT>::launch(in_row, grid, g, in, out, tb, s); \
+    if (g.bs_mode || g.map_mode) return FastExt<TYPE_, L_, A, B, C_, NT>::launch(in_row, grid, g, in, out, tb, s); \
     if (in_row)                                                                                  \
       k_fft_fast<TYPE_, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);      \
     else                                                                                         \

@@ -118,9 +118,20 @@ struct PassGeom {
   int bs_mode;
   int bs_logM;
   int64_t bs_L;
+  // Block map of a slab / pencil exchange fused into a specialised pass
+  // (bits; 0 = none): the pass reads its input (MAP_LOAD) or writes its
+  // output (MAP_STORE) in the per-peer block layout of the row-major array
+  // [map_outer][2^map_log_n][2^map_log_inner] instead of the natural layout,
+  // for an even partition of the n axis into blocks of 2^map_log_q: natural
+  // index v = (o*n + k)*inner + i lives in the block layout at
+  //   ((p*map_outer + o)*q + k % q)*inner + i,  p = k / q.
+  int map_mode;
+  int map_log_n, map_log_inner, map_log_q;
+  int64_t map_outer;
 };
 
 enum BsMode : int { BS_LOAD_MOD = 1, BS_STORE_MULH = 2, BS_STORE_DEMOD = 4 };
+enum MapMode : int { MAP_LOAD = 1, MAP_STORE = 2 };
 
 // Shared-memory row pitch (elements) of a generic-pass tile [L][pitch] whose
 // rows hold W columns.  Column-input passes put the W columns of a row on

@@ -814,6 +814,10 @@ struct Planner {
 
   // axes to transform (bit a = axis a); the others are batch axes
   uint64_t axes_mask = ~0ull;
+  // a plan that loads an exchange's block layout: axes in increasing order,
+  // one pass each (no transposing pair), with the first in-place step made
+  // the out-of-place one, so that the first step can take the load map
+  int load_first = 0;
 
   // SHAFFT_SM100_BS_FUSE=0 keeps Bluestein's element-wise steps as launches
   // of their own (for comparisons); by default they are fused into the
@@ -895,6 +899,17 @@ struct Planner {
     if (rotate_enabled && !tc_mode && all_axes && rotation_chain(out, ndim, dims)) return 0;
     int cur = BUF_SRC;
     int a = ndim - 1;
+    if (load_first) {
+      for (int b = 0; b < ndim; ++b) {
+        int64_t I = 1, O = 1;
+        for (int c = b + 1; c < ndim; ++c) I *= dims[c];
+        for (int c = 0; c < b; ++c) O *= dims[c];
+        if (!on(b)) continue;
+        int rc = axis(out, O, dims[b], I, cur, false, false);
+        if (rc) return rc;
+      }
+      a = -1;
+    }
     // the contiguous axis and its neighbour: two transposing passes when both
     // lengths have a specialised pass (every store is then a column tile)
     while (a >= 0 && !on(a)) --a;
@@ -940,9 +955,12 @@ struct Planner {
       return 0;
     }
     if (out.back().out_buf == BUF_DST) return 0;
-    // Parity fix: let the last in-place step write the other buffer instead,
-    // and exchange src/dst for every step after it.
-    for (int i = (int)out.size() - 1; i >= 0; --i) {
+    // Parity fix: let the last in-place step (the first, with load_first)
+    // write the other buffer instead, and exchange src/dst for every step
+    // after it.
+    const int nsteps = (int)out.size();
+    for (int it = 0; it < nsteps; ++it) {
+      const int i = load_first ? it : nsteps - 1 - it;
       Step& st = out[i];
       const bool user = (st.in_buf == BUF_SRC || st.in_buf == BUF_DST);
       const bool inplace_pass =
@@ -1021,6 +1039,7 @@ struct shafft_sm100_plan_s {
   int flags = 0;
   size_t off_tcerr = 0;  // device error word of passes with bounded waits (0 = ok)
   bool check_err = false;  // some pass may set it (tensor-core or column passes)
+  int map_fused = 0;       // exchange block maps fused: bit 0 load, bit 1 store
   // Replayed launch sequences: executes with the same (src, dst, direction,
   // scale) run as one CUDA graph from the third call on (the first runs
   // eagerly, the second is captured on a private stream).
@@ -1270,11 +1289,12 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
       snprintf(b, sizeof(b),
                "{\"kind\":\"pass\",\"L\":%d,\"radices\":[%s],\"W\":%d,\"in\":\"%s\",\"out\":\"%s\","
                "\"in_row\":%d,\"out_row\":%d,\"tiles\":%lld,\"smem\":%zu,\"twiddle\":%d,"
-               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d,\"tc\":%d,\"bs\":%d}",
+               "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d,\"tc\":%d,\"bs\":%d,"
+               "\"map\":%d}",
                st.g.L, rad.c_str(), st.g.W, buf_name(st.in_buf), buf_name(st.out_buf), st.g.in_row,
                st.g.out_row, (long long)st.g.ntiles, st.smem, st.g.tw_mode, (long long)st.g.ext[0],
                (long long)st.g.ext[1], (long long)st.g.ext[2], (long long)st.g.ext[3],
-               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast, st.tc, st.g.bs_mode);
+               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast, st.tc, st.g.bs_mode, st.g.map_mode);
     } else {
       const char* k = st.kind == ST_BS_MOD    ? "bluestein_modulate"
                       : st.kind == ST_BS_MULH ? "bluestein_multiply"
@@ -1339,8 +1359,109 @@ void configure(Planner& pl, const Knobs& k, uint64_t mask) {
   pl.widen = k.widen;
 }
 
+// Exchange block maps asked for a plan's input and output
+// (shafft_sm100_plan_create_axes_mapped): {outer, n, inner, parts} of the
+// [outer][n][inner] array whose per-peer blocks the input is read from /
+// the output is written to; parts = 0: none.
+struct BlockMaps {
+  int64_t load[4] = {0, 0, 0, 0};
+  int64_t store[4] = {0, 0, 0, 0};
+};
+
+static bool map_valid(const int64_t m[4], int64_t total) {
+  return m[0] >= 1 && m[2] >= 1 && m[3] >= 1 && m[1] >= m[3] && m[0] * m[1] * m[2] == total;
+}
+
+static int log2_exact(int64_t x) {
+  if (x < 1 || (x & (x - 1))) return -1;
+  int l = 0;
+  while (((int64_t)1 << l) < x) ++l;
+  return l;
+}
+
+// The fused form covers even partitions with power-of-two n, inner and
+// parts (index arithmetic by shifts); others keep the separate kernels.
+static bool map_fusable(const int64_t m[4]) {
+  return log2_exact(m[1]) >= 0 && log2_exact(m[2]) >= 0 && log2_exact(m[3]) >= 0;
+}
+
+static void set_map(PassGeom& g, const int64_t m[4], int bit) {
+  g.map_mode = bit;
+  g.map_outer = m[0];
+  g.map_log_n = log2_exact(m[1]);
+  g.map_log_inner = log2_exact(m[2]);
+  g.map_log_q = log2_exact(m[1] / m[3]);
+}
+
+// The loads or stores of a specialised pass take a block map when every
+// access the kernel makes to that buffer stays inside one run of `inner`
+// elements: 16-byte chunks of vw elements for column tiles (offsets that
+// are multiples of vw, inner a multiple of vw), whole rows of L points for
+// row tiles (offsets that are multiples of L, inner a multiple of L).
+static bool map_access_ok(const PassGeom& g, bool load, bool row_tile, int vw, int64_t inner) {
+  const int64_t unit = (load && row_tile) ? g.L : vw;
+  if (inner % unit) return false;
+  const int64_t* st = load ? g.sin : g.sout;
+  if (load && row_tile) {
+    if (g.sn_in != 1) return false;
+    for (int d = 0; d < 4; ++d)
+      if (g.ext[d] > 1 && st[d] % unit) return false;
+    return true;
+  }
+  if (st[0] != 1 || (load ? g.sn_in : g.sk_out) % unit) return false;
+  for (int d = 1; d < 4; ++d)
+    if (g.ext[d] > 1 && st[d] % unit) return false;
+  return true;
+}
+
+// Fuse the requested maps into the first step's loads and the last step's
+// stores where those are out-of-place specialised passes; returns the fused
+// bits.  A step carries one map, so a one-step plan takes the store map.
+static int apply_maps(std::vector<Step>& steps, const BlockMaps& m, int precision, int64_t total) {
+  if (steps.empty()) return 0;
+  const int vw = precision ? 1 : 2;
+  int fused = 0;
+  auto plain_fast = [](const Step& st) {
+    return st.kind == ST_PASS && st.fast && !st.tc && st.g.bs_mode == 0 && st.g.map_mode == 0;
+  };
+  Step& last = steps.back();
+  if (map_valid(m.store, total) && map_fusable(m.store) && plain_fast(last) && last.out_buf == BUF_DST &&
+      last.in_buf != BUF_DST && map_access_ok(last.g, false, last.fast_row, vw, m.store[2])) {
+    set_map(last.g, m.store, MAP_STORE);
+    fused |= 2;
+  }
+  Step& first = steps.front();
+  if (map_valid(m.load, total) && map_fusable(m.load) && plain_fast(first) && first.in_buf == BUF_SRC &&
+      first.out_buf != BUF_SRC && map_access_ok(first.g, true, first.fast_row, vw, m.load[2])) {
+    set_map(first.g, m.load, MAP_LOAD);
+    fused |= 1;
+  }
+  return fused;
+}
+
+// The steps of a plan asked for block maps (planning only): the default
+// planning, or the load_first one when it fuses more of the maps.
+static int plan_with_maps(Planner& pl, std::vector<Step>& steps, int ndim, const int64_t* dims, int precision,
+                          int flags, uint64_t mask, int64_t total, const Knobs& k, const BlockMaps& maps) {
+  int rc = pl.plan_nd(steps, ndim, dims);
+  if (rc || maps.load[3] == 0) return rc;
+  Planner pl2(precision, flags);
+  configure(pl2, k, mask);
+  pl2.load_first = 1;
+  std::vector<Step> steps2;
+  if (pl2.plan_nd(steps2, ndim, dims) == 0) {
+    std::vector<Step> t1 = steps, t2 = steps2;
+    const int f1 = apply_maps(t1, maps, precision, total), f2 = apply_maps(t2, maps, precision, total);
+    if (__builtin_popcount(f2) > __builtin_popcount(f1)) {
+      pl = std::move(pl2);
+      steps = std::move(steps2);
+    }
+  }
+  return 0;
+}
+
 int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int precision, int flags,
-                uint64_t mask, int64_t total, const Knobs& k) {
+                uint64_t mask, int64_t total, const Knobs& k, const BlockMaps* maps = nullptr) {
   flags = effective_flags(flags, k);
   std::unique_ptr<shafft_sm100_plan_s> p(new (std::nothrow) shafft_sm100_plan_s());
   if (!p) return set_err(SHAFFT_SM100_EALLOC, "host allocation failed");
@@ -1351,7 +1472,8 @@ int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int preci
   p->flags = flags;
   Planner pl(precision, flags);
   configure(pl, k, mask);
-  int rc = pl.plan_nd(p->steps, ndim, dims);
+  int rc = maps ? plan_with_maps(pl, p->steps, ndim, dims, precision, flags, mask, total, k, *maps)
+                : pl.plan_nd(p->steps, ndim, dims);
   if (rc) return rc;
   bool cluster_steps = false;
   for (const Step& st : p->steps) cluster_steps |= (st.kind == ST_PLANE && st.cluster);
@@ -1363,6 +1485,7 @@ int create_plan(shafft_sm100_plan* out, int ndim, const int64_t* dims, int preci
     rc = pl.plan_nd(p->steps, ndim, dims);
     if (rc) return rc;
   }
+  if (maps) p->map_fused = apply_maps(p->steps, *maps, precision, total);
   p->off_tcerr = pl.off_tcerr;
   p->check_err = (flags & (SHAFFT_SM100_PLAN_TENSOR_CORE | SHAFFT_SM100_PLAN_TC_PRIME_AXES)) != 0;
   for (const Step& st : p->steps)
@@ -1670,6 +1793,62 @@ int shafft_sm100_plan_create_axes(shafft_sm100_plan* out, int ndim, const int64_
   Knobs k;
   if (measure) k = measured_knobs(ndim, dims, precision, flags, mask, total);
   return create_plan(out, ndim, dims, precision, flags, mask, total, k);
+}
+
+int shafft_sm100_plan_create_axes_mapped(shafft_sm100_plan* out, int ndim, const int64_t* dims,
+                                         int precision, int flags, int naxes, const int* axes,
+                                         const int64_t* load_map, const int64_t* store_map, int* fused) {
+  if (!out) return set_err(SHAFFT_SM100_EINVAL, "null plan pointer");
+  *out = nullptr;
+  if (fused) *fused = 0;
+  int64_t total = 0;
+  int rc = validate_flags(flags, precision);
+  if (rc) return rc;
+  rc = validate_dims(ndim, dims, precision, &total);
+  if (rc) return rc;
+  uint64_t mask = 0;
+  rc = axes_mask(ndim, naxes, axes, &mask);
+  if (rc) return rc;
+  BlockMaps m;
+  for (int i = 0; i < 4; ++i) {
+    if (load_map) m.load[i] = load_map[i];
+    if (store_map) m.store[i] = store_map[i];
+  }
+  for (const int64_t* q : {m.load, m.store})
+    if (q[3] != 0 && !map_valid(q, total))
+      return set_err(SHAFFT_SM100_EINVAL, "block map {%lld, %lld, %lld, %lld} does not cover the %lld elements",
+                     (long long)q[0], (long long)q[1], (long long)q[2], (long long)q[3], (long long)total);
+  flags &= ~SHAFFT_SM100_PLAN_MEASURE;
+  rc = create_plan(out, ndim, dims, precision, flags, mask, total, Knobs{}, &m);
+  if (!rc && fused) *fused = (*out)->map_fused;
+  return rc;
+}
+
+int shafft_sm100_plan_query_mapped(int ndim, const int64_t* dims, int precision, int naxes, const int* axes,
+                                   const int64_t* load_map, const int64_t* store_map, char* buf, int buflen) {
+  int64_t total = 0;
+  int rc = validate_dims(ndim, dims, precision, &total);
+  if (rc) return rc;
+  uint64_t mask = 0;
+  rc = axes_mask(ndim, naxes, axes, &mask);
+  if (rc) return rc;
+  BlockMaps m;
+  for (int i = 0; i < 4; ++i) {
+    if (load_map) m.load[i] = load_map[i];
+    if (store_map) m.store[i] = store_map[i];
+  }
+  for (const int64_t* q : {m.load, m.store})
+    if (q[3] != 0 && !map_valid(q, total)) return set_err(SHAFFT_SM100_EINVAL, "block map does not cover the tensor");
+  Planner pl(precision, 0);
+  configure(pl, Knobs{}, mask);
+  std::vector<Step> steps;
+  rc = plan_with_maps(pl, steps, ndim, dims, precision, 0, mask, total, Knobs{}, m);
+  if (rc) return rc;
+  const int fused = apply_maps(steps, m, precision, total);
+  std::string d = describe_steps(precision, steps, total);
+  d.pop_back();  // the closing brace
+  d += ",\"fused\":" + std::to_string(fused) + "}";
+  return copy_out(d, buf, buflen);
 }
 
 int shafft_sm100_plan_create_1d(shafft_sm100_plan* out, int64_t n, int precision) {

@@ -14,8 +14,14 @@ everything on the device goes through the kernel library:
                  distributed axis b of that slot becomes contiguous and the
                  contiguous axis a = b + nca (nca = ndim - nda) becomes
                  distributed -- pack the local block along a into per-peer
-                 blocks (shafft_sm100_pack_blocks), all-to-all, unpack along
-                 b (skipped when b is the outermost axis)
+                 blocks, all-to-all, unpack along b (skipped when b is the
+                 outermost axis).  The pack is fused into the stores of the
+                 subplan before the exchange and the unpack into the loads of
+                 the subplan after it where the kernel library can
+                 (shafft_sm100_plan_create_axes_mapped: power-of-two shapes
+                 whose neighbouring step is an out-of-place specialised pass);
+                 otherwise they are separate kernels
+                 (shafft_sm100_pack_blocks / shafft_sm100_unpack_blocks)
   sequences      subplans alternate with ceil(nda / nca) sequences of up to
                  nca exchanges; after the last one the layout is
                  REDISTRIBUTED (TransformLayout INITIAL replays the exchanges
@@ -386,9 +392,20 @@ class FFTND:
             self.ops = CudaOps(self.precision)
         L = self.layout
         self.subplans = []
+        self._variants = {}
         if L.active:
             for s, idx in enumerate(L.plan_index):
                 self.subplans.append(self.ops.plan(L.sub[idx], L.tf_axes[s]))
+            # subplans with the neighbouring exchanges' packing fused, for
+            # every execute sequence the output policy leads to
+            starts = [(FORWARD, 0), (BACKWARD, L.nda)]
+            if self.output_policy == LAYOUT_INITIAL:
+                starts.append((BACKWARD, 0))
+            for direction, stage in starts:
+                seq = self._sequence(direction, stage)
+                for pos, op in enumerate(seq):
+                    if op[0] == "fft":
+                        self._variant(op[1], *self._maps(seq, pos))
         self.data = self.work = None
         self._state = "planned"
         return 0
@@ -396,7 +413,11 @@ class FFTND:
     def release(self):
         for p in getattr(self, "subplans", []):
             self.ops.destroy(p)
+        for v in getattr(self, "_variants", {}).values():
+            if v is not None:  # None: nothing was fused, the plain subplan served
+                self.ops.destroy(v[0])
         self.subplans = []
+        self._variants = {}
         self._state = "released"
 
     # buffers ---------------------------------------------------------------
@@ -441,27 +462,100 @@ class FFTND:
         return 0, list(self.layout.cas[s]), list(self.layout.das[s])
 
     # compute ---------------------------------------------------------------
-    def _fft(self, s, direction):
-        self.ops.execute(self.subplans[s], self.data, self.work, direction)
-        self.data, self.work = self.work, self.data
-
-    def _exchange(self, forward):
-        """One exchange from the current stage (forward: i = stage; backward:
-        i = stage - 1); the result is left in data."""
+    def _sequence(self, direction, stage):
+        """The steps of one execute that starts at `stage`, in order:
+        ("fft", s) runs subplan s; ("x", i, forward) is exchange i (stage i
+        <-> i + 1) in that direction."""
         L = self.layout
-        i = self.stage if forward else self.stage - 1
-        j, a, b, Q, pack, unpack, send, recv = L.exchange(i)
+        nes, seq = len(L.es), []
+        if direction == FORWARD:
+            for s in range(nes + 1):
+                seq.append(("fft", s))
+                if s < nes:
+                    for _ in range(L.es[s]):
+                        seq.append(("x", stage, True))
+                        stage += 1
+            if self.output_policy == LAYOUT_INITIAL:
+                while stage > 0:
+                    seq.append(("x", stage - 1, False))
+                    stage -= 1
+        else:
+            while stage < L.nda:  # re-apply the redistribution first
+                seq.append(("x", stage, True))
+                stage += 1
+            for s in range(nes, -1, -1):
+                seq.append(("fft", s))
+                if s > 0:
+                    for _ in range(L.es[s - 1]):
+                        seq.append(("x", stage - 1, False))
+                        stage -= 1
+        return seq
+
+    def _geometry(self, i, forward):
+        """(cart dim, parts, pack, unpack, send, recv) of exchange i in a
+        direction; pack / unpack = (outer, n, inner) of the block layout."""
+        j, a, b, Q, pack, unpack, send, recv = self.layout.exchange(i)
         if not forward:
             pack, unpack, send, recv = unpack, pack, recv, send
+        return j, Q, pack, unpack, send, recv
+
+    def _maps(self, seq, pos):
+        """Block maps to fuse into the subplan at seq[pos]: the unpack of the
+        exchange before it (its loads) and the pack of the exchange after it
+        (its stores), each (outer, n, inner, parts) or None when that side
+        needs no (un)packing."""
+        load = store = None
+        if pos > 0 and seq[pos - 1][0] == "x":
+            _, Q, _, unpack, _, _ = self._geometry(*seq[pos - 1][1:])
+            if unpack[0] != 1:
+                load = tuple(unpack) + (Q,)
+        if pos + 1 < len(seq) and seq[pos + 1][0] == "x":
+            _, Q, pack, _, _, _ = self._geometry(*seq[pos + 1][1:])
+            if pack[0] != 1:
+                store = tuple(pack) + (Q,)
+        return load, store
+
+    def _variant(self, s, load, store):
+        """(plan handle, fused bits) of subplan s with the maps fused where
+        the library can (bit 0: load, bit 1: store); the plain subplan when
+        there is nothing to fuse."""
+        if (load is None and store is None) or not hasattr(self.ops, "plan_mapped"):
+            return self.subplans[s], 0
+        key = (s, load, store)
+        if key not in self._variants:
+            L = self.layout
+            idx = L.plan_index[s]
+            h, fused = self.ops.plan_mapped(L.sub[idx], L.tf_axes[s], load, store)
+            if fused == 0:
+                self.ops.destroy(h)
+                h = self.subplans[s]
+                self._variants[key] = None
+                return h, 0
+            self._variants[key] = (h, fused)
+        v = self._variants[key]
+        return (self.subplans[s], 0) if v is None else v
+
+    def _fft(self, s, direction, load=None, store=None):
+        h, fused = self._variant(s, load, store)
+        self.ops.execute(h, self.data, self.work, direction)
+        self.data, self.work = self.work, self.data
+        return fused
+
+    def _exchange(self, i, forward, packed=False, leave_blocks=False):
+        """Exchange i in a direction; the result is left in data.  packed:
+        data already holds the per-peer blocks (the subplan before stored
+        them); leave_blocks: the received blocks stay unpacked (the subplan
+        after loads them through its map)."""
+        j, Q, pack, unpack, send, recv = self._geometry(i, forward)
         grp = self.lines.get(j, self.group)
-        if pack[0] == 1:  # blocks along the outermost axis are row ranges
+        if pack[0] == 1 or packed:  # outermost-axis blocks are row ranges already
             src = self.data
         else:
             self.ops.pack(self.data, self.work, *pack, Q)
             src = self.work
         dst = self.work if src is self.data else self.data
         self.ops.alltoall(dst, src, recv, send, grp, Q)
-        if unpack[0] == 1:
+        if unpack[0] == 1 or leave_blocks:
             if dst is not self.data:
                 self.data, self.work = self.work, self.data
         else:
@@ -480,26 +574,21 @@ class FFTND:
             return 0
         if self.data is None or self.work is None:
             return ERR_NO_BUFFER
-        nes = len(L.es)
-        if direction == FORWARD:
-            for s in range(nes + 1):
-                self._fft(s, FORWARD)
-                if s < nes:
-                    for _ in range(L.es[s]):
-                        self._exchange(True)
-            if self.output_policy == LAYOUT_INITIAL:
-                while self.stage > 0:
-                    self._exchange(False)
-        elif direction == BACKWARD:
-            while self.stage < L.nda:  # re-apply the redistribution first
-                self._exchange(True)
-            for s in range(nes, -1, -1):
-                self._fft(s, BACKWARD)
-                if s > 0:
-                    for _ in range(L.es[s - 1]):
-                        self._exchange(False)
-        else:
+        if direction not in (FORWARD, BACKWARD):
             return ERR_INVALID_STATE
+        seq = self._sequence(direction, self.stage)
+        # which subplans load / store the block layouts of their neighbours
+        fused = [0] * len(seq)
+        for pos, op in enumerate(seq):
+            if op[0] == "fft":
+                fused[pos] = self._variant(op[1], *self._maps(seq, pos))[1]
+        for pos, op in enumerate(seq):
+            if op[0] == "fft":
+                self._fft(op[1], direction, *self._maps(seq, pos))
+            else:
+                packed = pos > 0 and seq[pos - 1][0] == "fft" and bool(fused[pos - 1] & 2)
+                leave = pos + 1 < len(seq) and seq[pos + 1][0] == "fft" and bool(fused[pos + 1] & 1)
+                self._exchange(op[1], op[2], packed, leave)
         self.norm_exponent += 1
         return 0
 
@@ -749,6 +838,10 @@ class CudaOps:
         self.lib.shafft_sm100_plan_create_axes.argtypes = [
             ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        self.lib.shafft_sm100_plan_create_axes_mapped.argtypes = [
+            ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+            ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
         self.lib.shafft_sm100_twiddle_rows.argtypes = [
             ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
             ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
@@ -775,6 +868,20 @@ class CudaOps:
                                                                self.precision, 0, len(axes), a),
                         "plan_create_axes")
         return h
+
+    def plan_mapped(self, dims, axes, load_map, store_map):
+        """Subplan with exchange block maps (outer, n, inner, parts) fused
+        into its loads / stores where the library can: (handle, fused bits)."""
+        h = ctypes.c_void_p()
+        d = (ctypes.c_int64 * len(dims))(*dims)
+        a = (ctypes.c_int * len(axes))(*axes)
+        lm = None if load_map is None else (ctypes.c_int64 * 4)(*load_map)
+        sm = None if store_map is None else (ctypes.c_int64 * 4)(*store_map)
+        fused = ctypes.c_int(0)
+        self._sm._check(self.lib.shafft_sm100_plan_create_axes_mapped(
+            ctypes.byref(h), len(dims), d, self.precision, 0, len(axes), a, lm, sm, ctypes.byref(fused)),
+            "plan_create_axes_mapped")
+        return h, fused.value
 
     def destroy(self, h):
         self.lib.shafft_sm100_plan_destroy(h)

@@ -146,6 +146,28 @@ def test_error_state_is_thread_local():
     assert lib.shafftLastErrorStatus() == 0
 
 
+def test_planner_fuses_exchange_block_maps():
+    """Host-only planner: where a slab exchange's pack / unpack goes.  Forward
+    (store map, pack along axis 1 into 2 blocks): the last step, the column
+    pass of axis 1, writes the blocks.  Backward (load map): the plan starts
+    with that column pass, out of place, reading the blocks, and the row pass
+    of axis 2 follows in place.  Non-power-of-two maps stay separate."""
+    q = _sm100.plan_query_mapped([256, 512, 512], [1, 2], 0, None, (256, 512, 512, 2))
+    assert q["fused"] == 2 and [s["map"] for s in q["steps"]] == [0, 2]
+    assert q["steps"][-1]["fast"] == 1 and q["steps"][-1]["out"] == "dst"
+    q = _sm100.plan_query_mapped([256, 512, 512], [1, 2], 0, (256, 512, 512, 2), None)
+    assert q["fused"] == 1 and [s["map"] for s in q["steps"]] == [1, 0]
+    assert [(s["in"], s["out"]) for s in q["steps"]] == [("src", "dst"), ("dst", "dst")]
+    q = _sm100.plan_query_mapped([64, 64, 32], [1, 2], 1, (64, 64, 32, 4), None)
+    assert q["fused"] == 1
+    q = _sm100.plan_query_mapped([8, 48, 32], [1, 2], 0, None, (8, 48, 32, 2))
+    assert q["fused"] == 0 and all(s["map"] == 0 for s in q["steps"])
+    q = _sm100.plan_query_mapped([8, 64, 32], [1, 2], 0, None, (8, 64, 32, 3))  # uneven blocks
+    assert q["fused"] == 0
+    with pytest.raises(RuntimeError):
+        _sm100.plan_query_mapped([8, 64, 32], [1, 2], 0, None, (8, 64, 16, 2))  # wrong element count
+
+
 def test_planner_pass_lists():
     """Host-only planner: pass structure of the headline and config shapes."""
     # headline: transposing X and Y passes, then the Z column pass

@@ -27,18 +27,29 @@ from shafft_b200 import slab
 
 class NumpyOps:
     """Stand-in for the CUDA steps: numpy FFTs over axis subsets and the same
-    block layout as shafft_sm100_pack_blocks."""
-    def plan(self, dims, axes): return (tuple(dims), tuple(axes))
+    block layout as shafft_sm100_pack_blocks; plan_mapped fuses every block
+    map it is given (unpack before, pack after the FFT)."""
+    def plan(self, dims, axes): return (tuple(dims), tuple(axes), None, None)
+    def plan_mapped(self, dims, axes, load, store):
+        return (tuple(dims), tuple(axes), load, store), (1 if load else 0) | (2 if store else 0)
     def destroy(self, h): pass
     def execute(self, h, src, dst, direction):
-        dims, axes = h
+        dims, axes, load, store = h
         n = math.prod(dims)
+        if load:
+            tmp = torch.zeros(n, dtype=torch.complex128)
+            self.unpack(src, tmp, *load)
+            src = tmp
         x = src[:n].numpy().reshape(dims)
         if direction == S.FORWARD:
             y = np.fft.fftn(x, axes=axes)
         else:
             y = np.fft.ifftn(x, axes=axes) * math.prod(dims[a] for a in axes)
-        dst[:n] = torch.from_numpy(y.ravel())
+        y = torch.from_numpy(y.ravel().copy())
+        if store:
+            self.pack(y, dst, *store)
+        else:
+            dst[:n] = y
     def pack(self, src, dst, outer, n, inner, P):
         a = src[:outer * n * inner].numpy().reshape(outer, n, inner)
         parts = [a[:, s:s + l, :].ravel() for l, s in (slab.block_partition(n, P, p) for p in range(P))]
@@ -80,7 +91,16 @@ class NumpyOps:
         y[valid:] = 0
         dst[:count] = torch.from_numpy(y)
 
+class SeparateOps:
+    """The same steps without plan_mapped: every exchange packs and unpacks
+    with its own kernel."""
+    def __init__(self): self._o = NumpyOps()
+    def __getattr__(self, k):
+        if k == "plan_mapped": raise AttributeError(k)
+        return getattr(self._o, k)
+
 cfg = json.loads(sys.argv[3])
+make_ops = SeparateOps if cfg.get("separate") else NumpyOps
 dist.init_process_group("gloo")
 rank, world = dist.get_rank(), dist.get_world_size()
 if cfg.get("fft1d"):
@@ -116,9 +136,10 @@ rng = np.random.Generator(np.random.MT19937(5))
 g = rng.uniform(-1, 1, dims) + 1j * rng.uniform(-1, 1, dims)
 f = S.__dict__
 plan = slab.FFTND()
-rc = plan.init(cdims, dims, S.Z2Z, None, cfg["policy"], device_ops=NumpyOps())
+rc = plan.init(cdims, dims, S.Z2Z, None, cfg["policy"], device_ops=make_ops())
 assert rc == 0, rc
 assert plan.plan() == 0
+fused_variants = sum(1 for v in plan._variants.values() if v)
 n = plan.alloc_size()
 a = torch.zeros(max(n, 1), dtype=torch.complex128); b = torch.zeros_like(a)
 assert plan.set_buffers(a, b) == 0
@@ -141,7 +162,7 @@ back = d[:math.prod(sub)].numpy().reshape(sub)
 rt_err = float(np.abs(back - g[tuple(slice(o, o + s) for o, s in zip(off, sub))]).max()) if back.size else 0.0
 dist.destroy_process_group()
 json.dump({"rank": rank, "fwd_err": fwd_err, "rt_err": rt_err, "fwd_layout": [sub, off],
-           "axes": cur_axes}, open(sys.argv[2], "w"))
+           "axes": cur_axes, "fused_variants": fused_variants}, open(sys.argv[2], "w"))
 '''
 
 
@@ -166,13 +187,17 @@ def _run(tmp_path, world, cfg):
     return [json.loads((tmp_path / f"r{r}.json").read_text()) for r in range(world)]
 
 
+@pytest.mark.parametrize("separate", [False, True])
 @pytest.mark.parametrize("world,dims,policy", [
     (2, (6, 5, 7), 0), (2, (6, 5, 7), 1), (3, (7, 4, 5), 0), (3, (8, 6), 1), (2, (4, 3, 2, 5), 0)])
-def test_slab_fftnd_on_gloo_ranks(tmp_path, world, dims, policy):
-    res = _run(tmp_path, world, {"dims": list(dims), "P": world, "policy": policy})
+def test_slab_fftnd_on_gloo_ranks(tmp_path, world, dims, policy, separate):
+    """Both forms of the exchanges' packing: fused into the neighbouring
+    subplans (plan_mapped) and as separate pack / unpack steps."""
+    res = _run(tmp_path, world, {"dims": list(dims), "P": world, "policy": policy, "separate": separate})
     for o in res:
         assert o["fwd_err"] < 1e-12, o
         assert o["rt_err"] < 1e-12, o
+        assert (o["fused_variants"] == 0) == separate, o
 
 
 def test_inactive_rank_owns_nothing(tmp_path):
@@ -188,9 +213,10 @@ def test_inactive_rank_owns_nothing(tmp_path):
     (6, [2, 3, 1], (8, 6, 10), 0),        # unequal grid dimensions
     (4, [2, 2, 1, 1], (8, 6, 10, 4), 0),  # nca = 2: one sequence of two exchanges
     (5, [2, 2, 1], (6, 4, 5), 1)])        # one inactive rank
-def test_pencil_fftnd_on_gloo_ranks(tmp_path, world, comm_dims, dims, policy):
+@pytest.mark.parametrize("separate", [False, True])
+def test_pencil_fftnd_on_gloo_ranks(tmp_path, world, comm_dims, dims, policy, separate):
     res = _run(tmp_path, world, {"dims": list(dims), "P": comm_dims[0], "comm_dims": comm_dims,
-                                 "policy": policy})
+                                 "policy": policy, "separate": separate})
     for o in res:
         assert o["fwd_err"] < 1e-12, o
         assert o["rt_err"] < 1e-12, o
