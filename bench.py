@@ -1060,10 +1060,11 @@ def suite_tc(args):
 
 def exchange_rows(gpu, cases=((256, 2), (128, 4), (64, 8))):
     """The local device steps before a slab exchange of 512^3 complex64 on
-    P ranks (one rank's block of 512/P x 512 x 512, axes 1 and 2, then the
-    pack along axis 1 into P per-peer blocks): the plain subplan followed by
-    the separate pack kernel against the subplan with the pack fused into its
-    last pass's stores.  Both outputs are compared."""
+    P ranks (one rank's block of 512/P x 512 x 512: axes 1 and 2, then the
+    pack of the last axis into P per-peer blocks, the axis the exchange
+    distributes): the plain subplan followed by the separate pack kernel
+    against the subplan with the pack fused into its last pass's stores.
+    Both outputs are compared."""
     import torch
 
     from shafft_b200.slab import CudaOps
@@ -1077,11 +1078,11 @@ def exchange_rows(gpu, cases=((256, 2), (128, 4), (64, 8))):
         x0 = (torch.rand(2 * n, device="cuda", generator=g) * 2 - 1).view(torch.complex64)
         a, b, c = torch.empty_like(x0), torch.empty_like(x0), torch.empty_like(x0)
         h0 = ops.plan(dims, [1, 2])
-        h1, fused = ops.plan_mapped(dims, [1, 2], None, (m, 512, 512, parts))
+        h1, fused = ops.plan_mapped(dims, [1, 2], None, (m * 512, 512, 1, parts))
 
         def separate():
             ops.execute(h0, a, b, 0)
-            ops.pack(b, c, m, 512, 512, parts)
+            ops.pack(b, c, m * 512, 512, 1, parts)
 
         def fused_step():
             ops.execute(h1, a, b, 0)

@@ -96,7 +96,8 @@ int shafft_sm100_plan_create_axes(shafft_sm100_plan* out, int ndim, const int64_
  * block partition of shafft_sm100_pack_blocks.  A map is fused when n,
  * inner and parts are powers of two (even blocks) and the plan's first step
  * (load) or last step (store) is an out-of-place specialised pass whose
- * accesses stay inside runs of `inner` elements;
+ * accesses stay inside the runs the map keeps contiguous (a block's
+ * n / parts * inner elements);
  * *fused returns bit 0 = load map fused, bit 1 = store map fused (a one-step
  * plan takes only the store map).  A map that is not fused is not applied:
  * the caller packs or unpacks with shafft_sm100_pack_blocks /

@@ -195,7 +195,7 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
 #pragma unroll
         for (int e = 0; e < VW; ++e) {
           int64_t row = bin + (int64_t)(bc[b] * VW + e) * g.sin[0];
-          // a row of L points lies in one run of 2^map_log_inner (the planner checks)
+          // a row of L points lies in one contiguous run of the map (the planner checks)
           if ((EXT & EXT_MAP) && (g.map_mode & MAP_LOAD)) row = map_block(g, row);
           R.v[b][r][e] = (LDP == LD_L2) ? ld_l2(in + row + n) : ld_stream(in + row + n);
         }
@@ -218,7 +218,7 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
         }
       } else {
         int64_t off = bin + bc[b] * VW + (int64_t)n * g.sn_in;
-        if ((EXT & EXT_MAP) && (g.map_mode & MAP_LOAD)) off = map_block(g, off);  // a chunk lies in one run
+        if ((EXT & EXT_MAP) && (g.map_mode & MAP_LOAD)) off = map_block(g, off);  // a chunk stays contiguous
         const void* src = in + off;
         float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
@@ -437,7 +437,7 @@ __device__ __forceinline__ void fast_finish(const PassGeom& g, const typename Cx
         }
         if ((EXT & EXT_BS) && (g.bs_mode & BS_STORE_DEMOD)) continue;  // stored element-wise above
         int64_t off = bout + c * VW + (int64_t)k * g.sk_out;
-        if ((EXT & EXT_MAP) && (g.map_mode & MAP_STORE)) off = map_block(g, off);  // a chunk lies in one run
+        if ((EXT & EXT_MAP) && (g.map_mode & MAP_STORE)) off = map_block(g, off);  // a chunk stays contiguous
         float4* dstp = reinterpret_cast<float4*>(out + off);
         if (STP == ST_STREAM)
           st_chunk(dstp, *reinterpret_cast<float4*>(&ch));

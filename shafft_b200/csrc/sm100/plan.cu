@@ -1394,13 +1394,14 @@ static void set_map(PassGeom& g, const int64_t m[4], int bit) {
 }
 
 // The loads or stores of a specialised pass take a block map when every
-// access the kernel makes to that buffer stays inside one run of `inner`
-// elements: 16-byte chunks of vw elements for column tiles (offsets that
-// are multiples of vw, inner a multiple of vw), whole rows of L points for
-// row tiles (offsets that are multiples of L, inner a multiple of L).
-static bool map_access_ok(const PassGeom& g, bool load, bool row_tile, int vw, int64_t inner) {
+// access the kernel makes to that buffer stays inside one run that the map
+// keeps contiguous: q * inner consecutive elements (q = n / parts, the
+// block length), starting at a multiple of it.  The accesses are 16-byte
+// chunks of vw elements for column tiles (offsets that are multiples of vw)
+// and whole rows of L points for row tiles (offsets that are multiples of L).
+static bool map_access_ok(const PassGeom& g, bool load, bool row_tile, int vw, int64_t run) {
   const int64_t unit = (load && row_tile) ? g.L : vw;
-  if (inner % unit) return false;
+  if (run % unit) return false;
   const int64_t* st = load ? g.sin : g.sout;
   if (load && row_tile) {
     if (g.sn_in != 1) return false;
@@ -1426,13 +1427,13 @@ static int apply_maps(std::vector<Step>& steps, const BlockMaps& m, int precisio
   };
   Step& last = steps.back();
   if (map_valid(m.store, total) && map_fusable(m.store) && plain_fast(last) && last.out_buf == BUF_DST &&
-      last.in_buf != BUF_DST && map_access_ok(last.g, false, last.fast_row, vw, m.store[2])) {
+      last.in_buf != BUF_DST && map_access_ok(last.g, false, last.fast_row, vw, m.store[1] / m.store[3] * m.store[2])) {
     set_map(last.g, m.store, MAP_STORE);
     fused |= 2;
   }
   Step& first = steps.front();
   if (map_valid(m.load, total) && map_fusable(m.load) && plain_fast(first) && first.in_buf == BUF_SRC &&
-      first.out_buf != BUF_SRC && map_access_ok(first.g, true, first.fast_row, vw, m.load[2])) {
+      first.out_buf != BUF_SRC && map_access_ok(first.g, true, first.fast_row, vw, m.load[1] / m.load[3] * m.load[2])) {
     set_map(first.g, m.load, MAP_LOAD);
     fused |= 1;
   }

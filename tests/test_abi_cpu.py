@@ -152,6 +152,11 @@ def test_planner_fuses_exchange_block_maps():
     pass of axis 1, writes the blocks.  Backward (load map): the plan starts
     with that column pass, out of place, reading the blocks, and the row pass
     of axis 2 follows in place.  Non-power-of-two maps stay separate."""
+    # a 3-D slab exchange distributes the last axis: blocks of 512 / P points
+    q = _sm100.plan_query_mapped([256, 512, 512], [1, 2], 0, None, (256 * 512, 512, 1, 2))
+    assert q["fused"] == 2 and [s["map"] for s in q["steps"]] == [0, 2]
+    q = _sm100.plan_query_mapped([256, 512, 512], [1, 2], 0, (256 * 512, 512, 1, 2), None)
+    assert q["fused"] == 1 and [s["map"] for s in q["steps"]] == [1, 0]
     q = _sm100.plan_query_mapped([256, 512, 512], [1, 2], 0, None, (256, 512, 512, 2))
     assert q["fused"] == 2 and [s["map"] for s in q["steps"]] == [0, 2]
     assert q["steps"][-1]["fast"] == 1 and q["steps"][-1]["out"] == "dst"

@@ -30,7 +30,9 @@ def blocks_np(x, outer, n, inner, parts):
 
 # (dims, axes, map over the local block, which side, fused bit expected)
 CASES = [
-    ((8, 64, 32), [1, 2], (8, 64, 32, 2), "store", 2),      # slab: pack along axis 1 after axes 1, 2
+    ((8, 64, 32), [1, 2], (512, 32, 1, 2), "store", 2),     # slab: pack of the last axis after axes 1, 2
+    ((16, 64, 32), [1, 2], (1024, 32, 1, 4), "load", 1),    # slab backward: unpack of the last axis
+    ((8, 64, 32), [1, 2], (8, 64, 32, 2), "store", 2),      # pack along axis 1
     ((16, 128, 64), [1, 2], (16, 128, 64, 4), "store", 2),
     ((4, 32, 16, 32), [2, 3], (128, 16, 32, 8), "store", 2),
     ((64, 8, 32), [0], (1, 64, 256, 2), "load", 1),         # outer = 1: blocks are row ranges

@@ -127,7 +127,7 @@ def test_distributed_fftnd_two_ranks(tmp_path, dims, prec, policy):
     (2, [2, 1, 1], (64, 128, 64), S.C2C, S.LAYOUT_REDISTRIBUTED),
     (2, [2, 1, 1], (32, 64, 128), S.Z2Z, S.LAYOUT_INITIAL),
     (4, [4, 1, 1], (64, 64, 32), S.C2C, S.LAYOUT_INITIAL),
-    (2, [2, 1], (256, 512), S.C2C, S.LAYOUT_REDISTRIBUTED),
+    (2, [2, 1, 1], (128, 64, 256), S.C2C, S.LAYOUT_REDISTRIBUTED),
     (4, [2, 2, 1], (64, 32, 64), S.C2C, S.LAYOUT_REDISTRIBUTED),
     (4, [2, 2, 1, 1], (16, 32, 16, 32), S.Z2Z, S.LAYOUT_INITIAL)])
 def test_distributed_fftnd_fused_packing(tmp_path, world, comm_dims, dims, prec, policy):
