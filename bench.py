@@ -459,6 +459,9 @@ def ours(args):
     if world == 1 and not args.no_forms and dims == DIMS:
         out["configs"] = configs_rows(args, local) + [r2c_row(local)]
         out["forms"] = forms(args, local)
+        out["exchange"] = {"what": "one rank's device steps before a 512^3 complex64 slab exchange: "
+                                   "subplan + separate pack vs the pack fused into the subplan's stores",
+                           "rows": exchange_rows(local)}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
