@@ -5,11 +5,13 @@
 // <= 13, or <= 256 for the direct-DFT path) is a sequence of passes, one per
 // axis, src -> dst then in place on dst.  Every (transform, pass) is a "slot"
 // with a device descriptor (PassGeom + table pointers).  Work tickets are
-// handed out from one global counter in the order
-//     all tiles of pass 0 of every transform, then pass 1, then pass 2 ...
-// and a tile of pass p of transform t first waits until every tile of pass
-// p-1 of t has completed (per-slot counters, bounded wait).  Because every
-// ticket of pass p-1 precedes every ticket of pass p and tickets are only
+// handed out from one global counter.  The transforms are grouped into
+// windows of about 16 MiB, and the ticket order is software-pipelined over
+// them: stage s holds pass p of window s - p for every p, so a window's pass
+// p runs one stage after its pass p-1, while that data is still in L2.  A
+// tile of pass p of transform t first waits until every tile of pass p-1 of
+// t has completed (per-slot counters, bounded wait).  Because every ticket
+// of pass p-1 of t precedes every ticket of pass p of t and tickets are only
 // claimed by running CTAs, every wait ends; the bound only guards against a
 // fault elsewhere (it sets the batch's error flag and moves on).
 //
@@ -54,6 +56,8 @@ int bfail(int code, const char* fmt, ...) {
   } while (0)
 
 constexpr unsigned kBatchSpinLimit = 1u << 22;
+// transforms per ticket-order window, in bytes (SHAFFT_SM100_BATCH_WINDOW_MB)
+constexpr int64_t kBatchWindowBytes = int64_t(16) << 20;
 constexpr int64_t kBatchDirectMax = 256;
 
 template <typename C>
@@ -353,6 +357,8 @@ template <typename T>
 int batch_build(shafft_sm100_batch_s* b, int autotune) {
   using C = typename Vec2<T>::type;
   const size_t es = sizeof(C);
+  int64_t window_bytes = kBatchWindowBytes;
+  if (const char* e = getenv("SHAFFT_SM100_BATCH_WINDOW_MB")) window_bytes = (int64_t)atoll(e) << 20;
   // distinct lengths -> table offsets
   std::map<int64_t, LenTab> lens;
   size_t table_bytes = 0;
@@ -454,19 +460,41 @@ int batch_build(shafft_sm100_batch_s* b, int autotune) {
     }
     per_transform[t].back().last = 1;
   }
-  // order slots by (pass, transform)
+  // Ticket order.  The transforms are cut, in submission order, into
+  // windows of about window_bytes; stage s holds pass p of window s - p for
+  // every p, later passes first.  A window's next pass then follows its
+  // previous one by one stage, while that data is still in L2, and every
+  // slot still follows its previous pass in ticket order (the waits end).
+  // One window (window_bytes = 0) is the pass-major order.
   std::vector<HostSlot> order;
   std::vector<std::vector<int>> slot_of(b->count);
   int maxpass = 0;
   for (auto& v : per_transform) maxpass = std::max(maxpass, (int)v.size());
-  for (int p = 0; p < maxpass; ++p)
-    for (int t = 0; t < b->count; ++t)
-      if (p < (int)per_transform[t].size()) {
-        HostSlot hs = per_transform[t][p];
-        hs.prev = (p == 0) ? -1 : slot_of[t][p - 1];
-        slot_of[t].push_back((int)order.size());
-        order.push_back(hs);
+  std::vector<int> wbeg{0};
+  {
+    int64_t acc = 0;
+    for (int t = 0; t < b->count; ++t) {
+      acc += b->elements[t] * (int64_t)es;
+      if (window_bytes > 0 && acc >= window_bytes && t + 1 < b->count) {
+        wbeg.push_back(t + 1);
+        acc = 0;
       }
+    }
+    wbeg.push_back(b->count);
+  }
+  const int nwin = (int)wbeg.size() - 1;
+  for (int st = 0; st < nwin + maxpass - 1; ++st)
+    for (int p = maxpass - 1; p >= 0; --p) {
+      const int w = st - p;
+      if (w < 0 || w >= nwin) continue;
+      for (int t = wbeg[w]; t < wbeg[w + 1]; ++t)
+        if (p < (int)per_transform[t].size()) {
+          HostSlot hs = per_transform[t][p];
+          hs.prev = (p == 0) ? -1 : slot_of[t][p - 1];
+          slot_of[t].push_back((int)order.size());
+          order.push_back(hs);
+        }
+    }
   b->nslots = (int)order.size();
   std::vector<int64_t> start(order.size() + 1, 0);
   for (size_t i = 0; i < order.size(); ++i) start[i + 1] = start[i] + order[i].g.ntiles;
