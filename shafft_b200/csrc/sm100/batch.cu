@@ -21,6 +21,7 @@
 // file (SHAFFT_SM100_TUNE_CACHE, default ~/.cache/shafft_sm100_tune.txt).
 #include <cuda_runtime.h>
 #include <stdarg.h>
+#include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -58,10 +59,13 @@ int bfail(int code, const char* fmt, ...) {
 constexpr unsigned kBatchSpinLimit = 1u << 22;
 // transforms per ticket-order window, in bytes (SHAFFT_SM100_BATCH_WINDOW_MB)
 constexpr int64_t kBatchWindowBytes = int64_t(16) << 20;
+// largest batch (in tiles) given a ticket -> slot table (4 bytes a ticket)
+constexpr int64_t kMaxTicketTable = int64_t(1) << 26;
 constexpr int64_t kBatchDirectMax = 256;
 
+// 16-byte aligned so that a warp copies each slot's PassGeom as int4s
 template <typename C>
-struct SlotDesc {
+struct alignas(16) SlotDesc {
   PassGeom g;
   const C* twL;
   const uint16_t* p2k;
@@ -70,6 +74,7 @@ struct SlotDesc {
   int pass;
   int last;  // 1 for the transform's final pass
   int prev;  // slot of the same transform's previous pass, or -1
+  int need;  // tiles of that previous pass (its completion count)
 };
 
 bool smooth13(int64_t L) {
@@ -81,17 +86,38 @@ bool smooth13(int64_t L) {
 
 // complex64: at most 80 registers so that three CTAs share an SM (the tiles
 // are latency-bound; 116 registers allowed only two); complex128 unbounded
+// slot of ticket t: the ticket table when there is one, else the last slot
+// whose start <= t (binary search)
+__device__ __forceinline__ int ticket_slot(long long t, const int* tslot, const int64_t* start, int nslots) {
+  if (tslot) return tslot[t];
+  int lo = 0, hi = nslots - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= t)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// One CTA works through tickets until the counter passes the last one.
+// Thread 0 claims a ticket and finds its slot (a table lookup), waits for the
+// slot's previous pass, and warp 0 copies the slot's geometry to shared
+// memory with all its lanes.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1)
-    k_fft_batch(const SlotDesc<typename Cx<T>::type>* slots, const int64_t* start, int nslots,
+    k_fft_batch(const SlotDesc<typename Cx<T>::type>* slots, const int64_t* start, const int* tslot, int nslots,
                 typename Cx<T>::type* const* src, typename Cx<T>::type* const* dst, int* done,
                 unsigned long long* ticket, int* err, int conj, double scale, unsigned spin_limit) {
   using C = typename Cx<T>::type;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   C* sm = reinterpret_cast<C*>(smem_raw);
-  __shared__ PassGeom sg;
+  __shared__ __align__(16) PassGeom sg;
   __shared__ long long s_t;
   __shared__ int s_slot;
+  static_assert(sizeof(PassGeom) % 16 == 0 && sizeof(PassGeom) / 16 <= 32, "one int4 per lane");
+  static_assert(sizeof(SlotDesc<C>) % 16 == 0 && offsetof(SlotDesc<C>, g) == 0, "aligned slot geometry");
   const int64_t total = start[nslots];
   for (;;) {
     if (threadIdx.x == 0) {
@@ -99,19 +125,10 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1)
       s_t = t;
       int slot = -1;
       if (t < total) {
-        // last slot whose start <= t
-        int lo = 0, hi = nslots - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (start[mid] <= t)
-            lo = mid;
-          else
-            hi = mid - 1;
-        }
-        slot = lo;
+        slot = ticket_slot(t, tslot, start, nslots);
         const int pv = slots[slot].prev;
         if (pv >= 0) {
-          const int need = (int)slots[pv].g.ntiles;
+          const int need = slots[slot].need;
           unsigned it = 0;
           for (;;) {
             int v;
@@ -131,11 +148,15 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1)
     const int slot = s_slot;
     if (slot < 0) break;
     const SlotDesc<C>& d = slots[slot];
-    if (threadIdx.x == 0) {
-      sg = d.g;
-      sg.conj_in = (conj && d.pass == 0) ? 1 : 0;
-      sg.conj_out = (conj && d.last) ? 1 : 0;
-      sg.scale = d.last ? scale : 1.0;
+    if (threadIdx.x < 32) {
+      if (threadIdx.x < sizeof(PassGeom) / 16)
+        reinterpret_cast<int4*>(&sg)[threadIdx.x] = reinterpret_cast<const int4*>(&d.g)[threadIdx.x];
+      __syncwarp();
+      if (threadIdx.x == 0) {
+        sg.conj_in = (conj && d.pass == 0) ? 1 : 0;
+        sg.conj_out = (conj && d.last) ? 1 : 0;
+        sg.scale = d.last ? scale : 1.0;
+      }
     }
     __syncthreads();
     PassTables<C> tb{};
@@ -212,6 +233,7 @@ struct shafft_sm100_batch_s {
   unsigned char* d_tables = nullptr;  // twiddle + digit tables per distinct length
   void* d_slots = nullptr;
   int64_t* d_start = nullptr;
+  int* d_tslot = nullptr;  // slot of every ticket (null above kMaxTicketTable tickets)
   int* d_ctl = nullptr;  // [0..1] ticket, [2] error, [4..4+nslots) done counters
   void** d_src = nullptr;
   void** d_dst = nullptr;
@@ -535,9 +557,17 @@ int batch_build(shafft_sm100_batch_s* b, int autotune) {
     hd[i].pass = hs.pass;
     hd[i].last = hs.last;
     hd[i].prev = hs.prev;
+    hd[i].need = hs.prev >= 0 ? (int)order[hs.prev].g.ntiles : 0;
   }
   BCUDA(cudaMemcpy(b->d_slots, hd.data(), sizeof(SlotDesc<C>) * hd.size(), cudaMemcpyHostToDevice));
   BCUDA(cudaMemcpy(b->d_start, start.data(), sizeof(int64_t) * start.size(), cudaMemcpyHostToDevice));
+  if (b->tickets <= kMaxTicketTable) {
+    std::vector<int> ts((size_t)b->tickets);
+    for (size_t i = 0; i + 1 < start.size(); ++i)
+      for (int64_t t = start[i]; t < start[i + 1]; ++t) ts[(size_t)t] = (int)i;
+    BCUDA(cudaMalloc(&b->d_tslot, sizeof(int) * std::max<size_t>(ts.size(), 1)));
+    if (!ts.empty()) BCUDA(cudaMemcpy(b->d_tslot, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice));
+  }
   b->smem = std::max<size_t>(maxsmem, 16);
   BCUDA(cudaFuncSetAttribute(k_fft_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)std::max<size_t>(b->smem, 48 * 1024)));
@@ -561,7 +591,7 @@ int batch_launch(shafft_sm100_batch_s* b, int conj, double scale, cudaStream_t s
   using C = typename Vec2<T>::type;
   BCUDA(cudaMemsetAsync(b->d_ctl, 0, sizeof(int) * (4 + b->nslots), s));
   k_fft_batch<T><<<b->grid, kThreads, b->smem, s>>>(
-      reinterpret_cast<const SlotDesc<C>*>(b->d_slots), b->d_start, b->nslots,
+      reinterpret_cast<const SlotDesc<C>*>(b->d_slots), b->d_start, b->d_tslot, b->nslots,
       reinterpret_cast<C* const*>(b->d_src), reinterpret_cast<C* const*>(b->d_dst), b->d_ctl + 4,
       reinterpret_cast<unsigned long long*>(b->d_ctl), b->d_ctl + 2, conj, scale, b->wait_limit);
   BCUDA(cudaGetLastError());
@@ -573,6 +603,7 @@ void batch_free(shafft_sm100_batch_s* b) {
   cudaFree(b->d_tables);
   cudaFree(b->d_slots);
   cudaFree(b->d_start);
+  if (b->d_tslot) cudaFree(b->d_tslot);
   cudaFree(b->d_ctl);
   cudaFree(b->d_src);
   cudaFree(b->d_dst);
