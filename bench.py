@@ -1121,7 +1121,7 @@ def suite_exchange(args):
 
 
 def forms(args, gpu):
-    """The three north-star forms against the plain kernels on this GPU, each
+    """The three forms (tensor cores, batched, served) against the plain kernels on this GPU, each
     timing with its own clock record and its error against the oracle:
     tensor cores (one prime-axis shape, FFT1D 2^24), batched (C4) and
     served (C5, one offered load below saturation and one at it)."""
