@@ -10,8 +10,10 @@
 // transforms instead of stalling the queue.  Memory admission stays in
 // arrival order: a request that does not fit the budget holds back the ones
 // behind it.
-//   * device input/output buffers come from a stream-ordered memory pool
-//     (cudaMallocAsync / cudaFreeAsync), so freeing is ordered after the work;
+//   * device input/output buffers come from the server's own stream-ordered
+//     memory pool (cudaMallocFromPoolAsync / cudaFreeAsync), so freeing is
+//     ordered after the work; it reuses only blocks whose frees completed,
+//     so no request's stream waits on another's;
 //   * plans are kept resident per shape; requests of one shape that overlap
 //     share its instance when the plan has no scratch or control state
 //     (plan_shareable), and get instances of their own otherwise; idle
@@ -407,10 +409,26 @@ int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, in
   s->budget = budget_bytes;
   s->nstreams = streams;
   cudaError_t e = cudaGetDevice(&s->device);
-  if (e == cudaSuccess) e = cudaDeviceGetDefaultMemPool(&s->pool, s->device);
+  if (e == cudaSuccess) {
+    // the server's own pool: its settings do not leak into the process's
+    // default pool
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->device;
+    e = cudaMemPoolCreate(&s->pool, &props);
+  }
   if (e == cudaSuccess) {
     uint64_t keep = UINT64_MAX;  // keep freed blocks cached in the pool
     e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  if (e == cudaSuccess) {
+    // A request's buffers may reuse blocks whose frees have completed, but
+    // never a block still in use by another stream's request: with internal
+    // dependencies allowed, the pool would make a small request's stream
+    // wait for a large request on another stream to finish.
+    int no = 0;
+    e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
   }
   for (int i = 0; e == cudaSuccess && i < streams; ++i) {
     cudaStream_t st = nullptr;
@@ -421,6 +439,7 @@ int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, in
   if (e != cudaSuccess) {
     for (auto st : s->streams)
       if (st) cudaStreamDestroy(st);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
     return sfail(SHAFFT_SM100_ECUDA, "server set-up: %s", cudaGetErrorString(e));
   }
@@ -535,6 +554,7 @@ int shafft_sm100_server_destroy(shafft_sm100_server s) {
   }
   for (auto& kv : s->plans)
     for (auto& p : kv.second) shafft_sm100_plan_destroy(p->plan);
+  if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;
   return 0;
 }
