@@ -561,7 +561,10 @@ int batch_build(shafft_sm100_batch_s* b, int autotune) {
   }
   BCUDA(cudaMemcpy(b->d_slots, hd.data(), sizeof(SlotDesc<C>) * hd.size(), cudaMemcpyHostToDevice));
   BCUDA(cudaMemcpy(b->d_start, start.data(), sizeof(int64_t) * start.size(), cudaMemcpyHostToDevice));
-  if (b->tickets <= kMaxTicketTable) {
+  // SHAFFT_SM100_BATCH_TICKET_TABLE=0 leaves the table out (the binary
+  // search that batches above kMaxTicketTable tickets use)
+  const char* tt = getenv("SHAFFT_SM100_BATCH_TICKET_TABLE");
+  if (b->tickets <= kMaxTicketTable && !(tt && atoi(tt) == 0)) {
     std::vector<int> ts((size_t)b->tickets);
     for (size_t i = 0; i + 1 < start.size(); ++i)
       for (int64_t t = start[i]; t < start[i + 1]; ++t) ts[(size_t)t] = (int)i;

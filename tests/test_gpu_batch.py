@@ -89,3 +89,30 @@ def test_batch_wait_timeout_sets_error_and_context_stays_usable():
     y = dst.download().reshape(x.shape)
     b.status()
     assert o.rel_l2(y, o.fftn(x.astype(np.complex128))) <= tol(x.size, 0)
+
+
+@pytest.mark.parametrize("window_mb", ["0", "1"])
+def test_batch_ticket_lookup_and_window_forms_agree(monkeypatch, window_mb):
+    """The ticket -> slot table and the binary search over slot starts (the
+    form batches above 2^26 tiles use, forced here with
+    SHAFFT_SM100_BATCH_TICKET_TABLE=0), with pass-major tickets (window 0) and
+    1 MiB windows: the same tiles with the same arithmetic, so the results
+    are bit-identical, and they match the oracle."""
+    xs = [o.uniform_input(s, seed=30 + i, dtype=np.complex64) for i, s in enumerate(SHAPES)]
+    monkeypatch.setenv("SHAFFT_SM100_BATCH_WINDOW_MB", window_mb)
+    outs = []
+    for table in ("1", "0"):
+        monkeypatch.setenv("SHAFFT_SM100_BATCH_TICKET_TABLE", table)
+        b = _sm100.Batch(SHAPES, S.C2C, autotune=False)
+        src = [S.DeviceBuffer(x.size, S.C2C) for x in xs]
+        dst = [S.DeviceBuffer(x.size, S.C2C) for x in xs]
+        for x, d in zip(xs, src):
+            d.upload(x)
+        b.execute([d.ptr for d in src], [d.ptr for d in dst], 0, 1.0, 0)
+        b.status()
+        outs.append([d.download() for d in dst])
+        b.destroy()
+    for i, (x, y0, y1) in enumerate(zip(xs, *outs)):
+        assert np.array_equal(y0, y1), SHAPES[i]
+        ref = o.fftn(x.astype(np.complex128))
+        assert o.rel_l2(y0.reshape(x.shape), ref) <= tol(x.size, S.C2C), SHAPES[i]
