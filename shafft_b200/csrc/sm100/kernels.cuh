@@ -116,45 +116,95 @@ __host__ __device__ constexpr int ilog2c(int x) {
   return l;
 }
 
+// One output of a direct-DFT tile, with the pass's fused post-twiddle,
+// scale and output conjugation.
+template <typename T, typename C>
+__device__ __forceinline__ void direct_put(const PassGeom& g, const PassTables<C>& tb, C* out, C y, int k, int w,
+                                           int64_t bout, int64_t w0, int64_t tconst, T scale) {
+  if (g.tw_mode == TW_POST) {
+    const int64_t tt = (g.tw_dim == 0) ? (w0 + w) : tconst;
+    y = cmul(y, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * tt));
+  }
+  if (g.scale != 1.0) y = cscale(y, scale);
+  if (g.conj_out) y.y = -y.y;
+  out[bout + (int64_t)w * g.sout[0] + (int64_t)k * g.sk_out] = y;
+}
+
 // Direct DFT of the tile held in shared memory (natural order, [n][w] with
-// the given pitch): X[k] = sum_n x[n] w_L^{nk}, the exponent n*k reduced
-// modulo L incrementally.  Used for lengths with a prime factor above 13 when
-// L is small enough that O(L) work per output beats a Bluestein round trip.
+// the given pitch), X[k] = sum_n x[n] w^{nk} with w = exp(-2 pi i / L),
+// evaluated in pairs.  With s[n] = x[n] + x[L-n] and d[n] = x[n] - x[L-n]
+// for n = 1 .. h (h = (L-1)/2), and e_k = (-1)^k x[L/2] for even L (0 for
+// odd L):
+//   X[k]   = x[0] + e_k + sum_n s[n] Re w^{nk} + i sum_n d[n] Im w^{nk}
+//   X[L-k] = x[0] + e_k + sum_n s[n] Re w^{nk} - i sum_n d[n] Im w^{nk}
+// for k = 1 .. h; X[0] = x[0] + sum_n s[n] + x[L/2] and, for even L,
+// X[L/2] = x[0] + sum_n (-1)^n s[n] + (-1)^{L/2} x[L/2].  Each table read
+// and each pair of real multiplies then serves two outputs, a quarter of
+// the arithmetic of the plain sum; the exponent n*k is reduced modulo L
+// incrementally.  Used for lengths with a prime factor above 13 when L is
+// small enough that O(L) work per output beats a Bluestein round trip.
 // Outputs go straight to HBM with the pass's fused twiddle/scale/conj.
 template <typename T, typename C>
-__device__ __forceinline__ void direct_store(const PassGeom& g, const PassTables<C>& tb, const C* sm,
-                                             C* out, int L, int W, int logW, int pitch, int wcount,
-                                             int64_t bout, int64_t w0, int64_t tconst) {
-  const int total = L << logW;
+__device__ __forceinline__ void direct_store(const PassGeom& g, const PassTables<C>& tb, C* sm, C* out, int L,
+                                             int W, int logW, int pitch, int wcount, int64_t bout, int64_t w0,
+                                             int64_t tconst) {
+  const int h = (L - 1) / 2;
+  const bool even = (L & 1) == 0;
+  // s and d in place: row n <- s[n], row L-n <- d[n]
+  for (int b = threadIdx.x; b < (h << logW); b += kThreads) {
+    const int w = b & (W - 1), n = 1 + (b >> logW);
+    const C a = sm[n * pitch + w], c = sm[(L - n) * pitch + w];
+    sm[n * pitch + w] = C{a.x + c.x, a.y + c.y};
+    sm[(L - n) * pitch + w] = C{a.x - c.x, a.y - c.y};
+  }
+  __syncthreads();
   const T scale = (T)g.scale;
-  for (int b = threadIdx.x; b < total; b += kThreads) {
-    int w, k;
-    if (g.out_row) {
-      k = b % L;
-      w = b / L;
-    } else {
-      w = b & (W - 1);
-      k = b >> logW;
-    }
+  // item (j, w): j = 0 gives X[0] (and X[L/2] for even L), j = 1 .. h gives
+  // X[j] and X[L-j]
+  const int items = (h + 1) << logW;
+  for (int b = threadIdx.x; b < items; b += kThreads) {
+    const int w = b & (W - 1), j = b >> logW;
     if (w >= wcount) continue;
-    T ar = 0, ai = 0;
+    const C x0 = sm[w];
+    const C xh = even ? sm[(L / 2) * pitch + w] : C{0, 0};
+    if (j == 0) {
+      C y0 = x0, yh = x0;
+      T sg = -1;
+      for (int n = 1; n <= h; ++n) {
+        const C sn = sm[n * pitch + w];
+        y0.x += sn.x;
+        y0.y += sn.y;
+        yh.x += sg * sn.x;
+        yh.y += sg * sn.y;
+        sg = -sg;
+      }
+      y0.x += xh.x;
+      y0.y += xh.y;
+      direct_put<T, C>(g, tb, out, y0, 0, w, bout, w0, tconst, scale);
+      if (even) {
+        const T e = ((L / 2) & 1) ? (T)-1 : (T)1;
+        yh.x += e * xh.x;
+        yh.y += e * xh.y;
+        direct_put<T, C>(g, tb, out, yh, L / 2, w, bout, w0, tconst, scale);
+      }
+      continue;
+    }
+    T px = 0, py = 0, qx = 0, qy = 0;
     int m = 0;
-    for (int n = 0; n < L; ++n) {
-      const C x = sm[n * pitch + w];
-      const C t = tb.twL[m];
-      ar += x.x * t.x - x.y * t.y;
-      ai += x.x * t.y + x.y * t.x;
-      m += k;
+    for (int n = 1; n <= h; ++n) {
+      m += j;
       if (m >= L) m -= L;
+      const C t = tb.twL[m];
+      const C sn = sm[n * pitch + w], dn = sm[(L - n) * pitch + w];
+      px += sn.x * t.x;
+      py += sn.y * t.x;
+      qx += dn.x * t.y;
+      qy += dn.y * t.y;
     }
-    C y = C{ar, ai};
-    if (g.tw_mode == TW_POST) {
-      const int64_t tt = (g.tw_dim == 0) ? (w0 + w) : tconst;
-      y = cmul(y, tw_n(tb, g.tw_shift, g.tw_mask, (int64_t)k * tt));
-    }
-    if (g.scale != 1.0) y = cscale(y, scale);
-    if (g.conj_out) y.y = -y.y;
-    out[bout + (int64_t)w * g.sout[0] + (int64_t)k * g.sk_out] = y;
+    const T e = (j & 1) ? (T)-1 : (T)1;
+    const T bx = x0.x + e * xh.x + px, by = x0.y + e * xh.y + py;
+    direct_put<T, C>(g, tb, out, C{bx - qy, by + qx}, j, w, bout, w0, tconst, scale);
+    direct_put<T, C>(g, tb, out, C{bx + qy, by - qx}, L - j, w, bout, w0, tconst, scale);
   }
 }
 
