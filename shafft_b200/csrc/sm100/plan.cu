@@ -157,7 +157,15 @@ static Limits limits_for(int precision) {
 }
 
 // longest non-smooth length handled by a direct-DFT pass
-constexpr int64_t kDirectMax = 128;
+constexpr int64_t kDirectMax = 256;
+// longest direct-DFT pass (SHAFFT_SM100_DIRECT_MAX overrides, up to 256)
+static int64_t direct_max() {
+  if (const char* e = getenv("SHAFFT_SM100_DIRECT_MAX")) {
+    const int64_t v = atoll(e);
+    if (v >= 0 && v <= 256) return v;
+  }
+  return kDirectMax;
+}
 
 static bool is_smooth(int64_t L) {
   const int64_t primes[] = {2, 3, 5, 7, 11, 13};
@@ -727,7 +735,7 @@ struct Planner {
     if (in_bluestein) return SHAFFT_SM100_ENOTSUP;
     // short lengths with a large prime factor: one direct-DFT pass (O(L)
     // work per output) instead of the five Bluestein steps
-    if (L <= kDirectMax) {
+    if (L <= direct_max()) {
       int ob = force_oop ? other_buf(cur) : cur;
       single_pass(out, O, (int)L, I, cur, ob);
       cur = ob;
