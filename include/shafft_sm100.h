@@ -183,7 +183,7 @@ int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen);
  *
  * count transforms; transform i has ndims[i] axes whose lengths follow in
  * `dims` (flattened, row-major, last axis fastest).  Every axis length must
- * factor into 2,3,5,7,11,13 and be <= 4096, or be <= 256 (direct DFT).
+ * factor into 2,3,5,7,11,13 and be <= 4096, or be <= 362 (direct DFT).
  * flags bit 0: autotune tile widths for lengths not yet in the tuning cache
  * (file SHAFFT_SM100_TUNE_CACHE, default ~/.cache/shafft_sm100_tune.txt).
  * execute: src[i] -> dst[i] for every i (device pointers; src[i] is only

@@ -2,7 +2,7 @@
 // in ONE persistent kernel launch, replayed from a captured CUDA graph.
 //
 // Each transform (any rank, every axis of length <= 4096 with prime factors
-// <= 13, or <= 256 for the direct-DFT path) is a sequence of passes, one per
+// <= 13, or <= 362 for the direct-DFT path) is a sequence of passes, one per
 // axis, src -> dst then in place on dst.  Every (transform, pass) is a "slot"
 // with a device descriptor (PassGeom + table pointers).  Work tickets are
 // handed out from one global counter.  The transforms are grouped into
@@ -61,7 +61,7 @@ constexpr unsigned kBatchSpinLimit = 1u << 22;
 constexpr int64_t kBatchWindowBytes = int64_t(16) << 20;
 // largest batch (in tiles) given a ticket -> slot table (4 bytes a ticket)
 constexpr int64_t kMaxTicketTable = int64_t(1) << 26;
-constexpr int64_t kBatchDirectMax = 256;
+constexpr int64_t kBatchDirectMax = 362;  // the plans' direct-DFT range (plan.cu)
 
 // 16-byte aligned so that a warp copies each slot's PassGeom as int4s
 template <typename C>
@@ -77,6 +77,12 @@ struct alignas(16) SlotDesc {
   int need;  // tiles of that previous pass (its completion count)
 };
 
+int pow2_floor(int x) {
+  int p = 1;
+  while (p * 2 <= x) p *= 2;
+  return p;
+}
+
 bool smooth13(int64_t L) {
   const int64_t primes[] = {2, 3, 5, 7, 11, 13};
   for (int64_t p : primes)
@@ -84,8 +90,6 @@ bool smooth13(int64_t L) {
   return L == 1;
 }
 
-// complex64: at most 80 registers so that three CTAs share an SM (the tiles
-// are latency-bound; 116 registers allowed only two); complex128 unbounded
 // slot of ticket t: the ticket table when there is one, else the last slot
 // whose start <= t (binary search)
 __device__ __forceinline__ int ticket_slot(long long t, const int* tslot, const int64_t* start, int nslots) {
@@ -105,6 +109,8 @@ __device__ __forceinline__ int ticket_slot(long long t, const int* tslot, const 
 // Thread 0 claims a ticket and finds its slot (a table lookup), waits for the
 // slot's previous pass, and warp 0 copies the slot's geometry to shared
 // memory with all its lanes.
+// complex64: at most 80 registers so that three CTAs share an SM (the tiles
+// are latency-bound; 116 registers allowed only two); complex128 unbounded
 template <typename T>
 __global__ void __launch_bounds__(kThreads, sizeof(T) == 4 ? 3 : 1)
     k_fft_batch(const SlotDesc<typename Cx<T>::type>* slots, const int64_t* start, const int* tslot, int nslots,
@@ -420,14 +426,15 @@ int batch_build(shafft_sm100_batch_s* b, int autotune) {
       const bool row = (I == 1);
       int W;
       if (row) {
-        const int def = (int)std::min<int64_t>(32, std::max<int64_t>(1, 8192 / L));
+        // tile widths are powers of two (the tile walks columns by mask and shift)
+        const int def = pow2_floor((int)std::min<int64_t>(32, std::max<int64_t>(1, 8192 / L)));
         W = tune_width<T>(L, true, O, def, es, autotune);
         g.ext[0] = O;
         g.sin[0] = g.sout[0] = L;
         g.ext[1] = g.ext[2] = g.ext[3] = 1;
         g.sn_in = g.sk_out = 1;
       } else {
-        const int def = (int)std::min<int64_t>(16, std::max<int64_t>(1, 8192 / L));
+        const int def = pow2_floor((int)std::min<int64_t>(16, std::max<int64_t>(1, 8192 / L)));
         W = tune_width<T>(L, false, I, def, es, autotune);
         g.ext[0] = I;
         g.sin[0] = g.sout[0] = 1;

@@ -157,12 +157,12 @@ static Limits limits_for(int precision) {
 }
 
 // longest non-smooth length handled by a direct-DFT pass
-constexpr int64_t kDirectMax = 256;
-// longest direct-DFT pass (SHAFFT_SM100_DIRECT_MAX overrides, up to 256)
+constexpr int64_t kDirectMax = 1024;
+// longest direct-DFT pass (SHAFFT_SM100_DIRECT_MAX overrides, up to 1024)
 static int64_t direct_max() {
   if (const char* e = getenv("SHAFFT_SM100_DIRECT_MAX")) {
     const int64_t v = atoll(e);
-    if (v >= 0 && v <= 256) return v;
+    if (v >= 0 && v <= 1024) return v;
   }
   return kDirectMax;
 }
@@ -733,9 +733,15 @@ struct Planner {
       }
     }
     if (in_bluestein) return SHAFFT_SM100_ENOTSUP;
-    // short lengths with a large prime factor: one direct-DFT pass (O(L)
-    // work per output) instead of the five Bluestein steps
-    if (L <= direct_max()) {
+    // short lengths with a large prime factor: one direct-DFT pass instead
+    // of the five Bluestein steps.  The paired direct DFT costs about L / 4
+    // multiply-adds per point, Bluestein a few passes over M >= 2L - 1
+    // points; measured on B200 (rows of 131 .. 1021 points) the direct pass
+    // wins while L^2 <= 128 M, which holds for every L up to 362 and for
+    // none above (from 513 on, M = 2048 pads too little to pay).
+    int64_t Mb = 1;
+    while (Mb < 2 * L - 1) Mb <<= 1;
+    if (L <= direct_max() && L * L <= 128 * Mb) {
       int ob = force_oop ? other_buf(cur) : cur;
       single_pass(out, O, (int)L, I, cur, ob);
       cur = ob;

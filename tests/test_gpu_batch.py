@@ -12,7 +12,8 @@ from shafft_b200 import _sm100
 pytestmark = pytest.mark.gpu
 
 SHAPES = [(16, 16), (64, 32, 8), (97, 24), (131, 5, 7), (211, 16), (12, 10, 14), (256, 256), (5,),
-          (1, 1), (63, 47, 31), (1000,), (4096, 3), (7, 11, 13), (2, 128, 2), (128, 1, 64), (243, 25)]
+          (1, 1), (63, 47, 31), (1000,), (4096, 3), (7, 11, 13), (2, 128, 2), (128, 1, 64), (243, 25),
+          (331, 3), (17, 353), (700,), (600, 5)]
 
 
 def tol(n, prec):
