@@ -62,6 +62,10 @@ constexpr int64_t kBatchWindowBytes = int64_t(16) << 20;
 // largest batch (in tiles) given a ticket -> slot table (4 bytes a ticket)
 constexpr int64_t kMaxTicketTable = int64_t(1) << 26;
 constexpr int64_t kBatchDirectMax = 362;  // the plans' direct-DFT range (plan.cu)
+// tile widths (batch columns a tile holds): the autotuner's range and the
+// defaults of axes it has not timed
+constexpr int kBatchRowWMax = 256, kBatchColWMax = 64;
+constexpr int kBatchRowWDefault = 256, kBatchColWDefault = 64;
 
 // 16-byte aligned so that a warp copies each slot's PassGeom as int4s
 template <typename C>
@@ -265,8 +269,11 @@ template <typename T>
 int tune_width(int64_t L, bool row, int64_t ext0, int default_w, size_t es, int autotune) {
   const int maxw_smem = (int)std::max<int64_t>(1, (96 * 1024) / ((L + 1) * (int64_t)es));
   std::vector<int> cands;
-  for (int w = 1; w <= 32; w *= 2) {
-    if (w > maxw_smem) break;
+  // widest tiles: 256 for rows, 64 for columns (the synthetic column tensor
+  // has 64 columns), and at most 8192 points a tile
+  const int wmax = row ? kBatchRowWMax : kBatchColWMax;
+  for (int w = 1; w <= wmax; w *= 2) {
+    if (w > maxw_smem || (w > 1 && (int64_t)w * L > 8192)) break;
     if (!row && w < 4 && ext0 >= 4) continue;
     if (w > 1 && w / 2 >= ext0) break;
     cands.push_back(w);
@@ -427,14 +434,14 @@ int batch_build(shafft_sm100_batch_s* b, int autotune) {
       int W;
       if (row) {
         // tile widths are powers of two (the tile walks columns by mask and shift)
-        const int def = pow2_floor((int)std::min<int64_t>(32, std::max<int64_t>(1, 8192 / L)));
+        const int def = pow2_floor((int)std::min<int64_t>(kBatchRowWDefault, std::max<int64_t>(1, 8192 / L)));
         W = tune_width<T>(L, true, O, def, es, autotune);
         g.ext[0] = O;
         g.sin[0] = g.sout[0] = L;
         g.ext[1] = g.ext[2] = g.ext[3] = 1;
         g.sn_in = g.sk_out = 1;
       } else {
-        const int def = pow2_floor((int)std::min<int64_t>(16, std::max<int64_t>(1, 8192 / L)));
+        const int def = pow2_floor((int)std::min<int64_t>(kBatchColWDefault, std::max<int64_t>(1, 8192 / L)));
         W = tune_width<T>(L, false, I, def, es, autotune);
         g.ext[0] = I;
         g.sin[0] = g.sout[0] = 1;
@@ -445,7 +452,7 @@ int batch_build(shafft_sm100_batch_s* b, int autotune) {
       }
       // never wider than the batch dimension rounded up to a power of two
       int cap = 1;
-      while (cap < g.ext[0] && cap < 32) cap *= 2;
+      while (cap < g.ext[0] && cap < kBatchRowWMax) cap *= 2;
       W = std::max(1, std::min(W, cap));
       g.W = W;
       g.logW = 0;
