@@ -173,6 +173,29 @@ def test_planner_fuses_exchange_block_maps():
         _sm100.plan_query_mapped([8, 64, 32], [1, 2], 0, None, (8, 64, 16, 2))  # wrong element count
 
 
+def test_planner_direct_dft_range():
+    """Host-only planner: an axis with a prime factor above 13 is one direct
+    DFT pass while L^2 <= 128 M (M the Bluestein length: every L up to 362),
+    Bluestein beyond; SHAFFT_SM100_DIRECT_MAX caps the direct range."""
+    def kinds(dims, prec=0):
+        return [s["kind"] for s in _sm100.plan_query(list(dims), prec)["steps"]]
+    for L in (17, 131, 257, 263, 331, 353, 362):
+        assert kinds([L]) == ["pass"], L
+    for L in (367, 383, 509, 1021):
+        assert kinds([L])[0] == "bluestein_modulate", L
+    assert kinds([5, 353], 1) == ["pass", "pass"]
+    old = os.environ.get("SHAFFT_SM100_DIRECT_MAX")
+    try:
+        os.environ["SHAFFT_SM100_DIRECT_MAX"] = "128"
+        assert kinds([131])[0] == "bluestein_modulate"
+        assert kinds([127]) == ["pass"]
+    finally:
+        if old is None:
+            del os.environ["SHAFFT_SM100_DIRECT_MAX"]
+        else:
+            os.environ["SHAFFT_SM100_DIRECT_MAX"] = old
+
+
 def test_planner_pass_lists():
     """Host-only planner: pass structure of the headline and config shapes."""
     # headline: transposing X and Y passes, then the Z column pass
