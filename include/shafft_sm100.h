@@ -286,8 +286,9 @@ int shafft_sm100_chirp_multiply(const void* src, void* dst, const void* factors,
  *                spectrum, so c2r(r2c(x)) = N x for N = prod(dims)
  * Both read their input as scratch (its contents are undefined afterwards);
  * buffers are 16-byte aligned device memory, input and output distinct.
- * The plan owns about 1.5x the spectrum's bytes of scratch.  Asynchronous on
- * `stream`. */
+ * The plan owns a work array of prod(dims) / 2 complex elements (the
+ * half-length complex view's transform) besides its C2C plan.  Asynchronous
+ * on `stream`. */
 typedef struct shafft_sm100_rplan_s* shafft_sm100_rplan;
 int shafft_sm100_rplan_create(shafft_sm100_rplan* out, int ndim, const int64_t* dims, int precision);
 int shafft_sm100_rplan_destroy(shafft_sm100_rplan plan);
