@@ -18,11 +18,13 @@
 //     share its instance when the plan has no scratch or control state
 //     (plan_shareable), and get instances of their own otherwise; idle
 //     instances are evicted oldest-first when the budget needs their memory;
-//   * each admitted request is issued on the least recently used of S streams
-//     (H2D copy, execute, D2H copy, frees), so requests that arrive while
+//   * each admitted request is issued on the one of S streams with the
+//     fewest bytes in flight (H2D copy, execute, D2H copy, frees), so that it
+//     does not queue behind a large request, and requests that arrive while
 //     others run overlap with them on the GPU; the copies go in pieces of
 //     8 MiB so that a small request's copy need not wait behind a whole large
-//     transfer on a copy engine.
+//     transfer on a copy engine; requests with buffers of 256 MiB or more
+//     copy in turn with each other, one per direction at a time.
 // A completion thread polls the per-request events, releases the budget and
 // the plan instance, stamps the completion time and wakes waiters.  Latency
 // is completion time minus submission time; statistics report p50 / p99.
@@ -78,7 +80,7 @@ struct Request {
   const void* host_in = nullptr;
   void* host_out = nullptr;
   size_t bytes = 0;  // one buffer
-  Clock::time_point t_submit, t_done;
+  Clock::time_point t_submit, t_issue, t_done;
   // in flight
   void* d_in = nullptr;
   void* d_out = nullptr;
@@ -99,6 +101,7 @@ struct shafft_sm100_server_s {
   int nstreams = 0;
   std::vector<cudaStream_t> streams;
   std::vector<Clock::time_point> stream_last;
+  std::vector<size_t> stream_bytes;  // device bytes of the requests in flight on each stream
   cudaMemPool_t pool = nullptr;
   int device = 0;
   std::mutex mu;
@@ -109,15 +112,20 @@ struct shafft_sm100_server_s {
   std::map<std::string, std::vector<std::unique_ptr<PlanInst>>> plans;
   size_t plan_bytes = 0;
   std::atomic<bool> stop{false};
+  std::atomic<bool> dispatch_done{false};  // the dispatcher has issued its last request
   std::thread dispatcher, completer;
   uint64_t next_id = 1;
   std::vector<double> latencies_ms;
+  std::vector<double> admit_ms;  // submission to the start of issue, per completed request
   Clock::time_point t_first, t_last;
   uint64_t completed = 0, failed = 0;
   int max_inflight_seen = 0;
   // plan-instance churn: creations (and their wall time) and evictions
   uint64_t plans_created = 0, plans_evicted = 0;
   double create_ms_total = 0, create_ms_max = 0;
+  // wall time of the dispatcher's CUDA calls for one request (allocation,
+  // copies, transform launches) or one round of pump steps: the longest
+  double issue_ms_max = 0;
   // background plan creation: shapes waiting for an instance (one build in
   // flight per shape)
   struct BuildJob {
@@ -129,6 +137,17 @@ struct shafft_sm100_server_s {
   std::map<std::string, int> building;
   std::condition_variable cv_build;
   std::thread builder;
+  // Large requests (kLargeCopy bytes a buffer or more) copy one at a time in
+  // each direction, in admission order: each waits for the previous large
+  // request's copy in the same direction (these events, recorded after it).
+  cudaEvent_t large_h2d = nullptr, large_d2h = nullptr;
+  // Copies of the requests issued whole (below kLargeCopy) not yet known to
+  // be done, one event each, per direction (dispatcher thread only).  The
+  // copy engines do not interleave another stream's copy with a large copy
+  // that keeps being fed (measured on B200: a 1 MiB copy waited 13 ms behind
+  // a 906 MiB copy fed two 8 MiB pieces at a time), so a pump holds its next
+  // piece back while one of these is pending.
+  std::deque<cudaEvent_t> small_h2d, small_d2h;
 };
 
 namespace {
@@ -253,6 +272,10 @@ void evict_idle(shafft_sm100_server_s* s, size_t need, const std::string& keep_k
 // of a large transfer already queued on the copy engine instead of after the
 // whole transfer.
 constexpr size_t kCopyChunk = size_t(8) << 20;
+// a request whose buffers are this large copies in turn with the other large
+// ones (two overlapping large copies would both take twice as long; in turn,
+// the first one is done at full speed and the second no later)
+constexpr size_t kLargeCopy = size_t(256) << 20;
 cudaError_t copy_chunked(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, cudaStream_t st) {
   for (size_t off = 0; off < bytes; off += kCopyChunk) {
     const size_t n = bytes - off < kCopyChunk ? bytes - off : kCopyChunk;
@@ -263,12 +286,172 @@ cudaError_t copy_chunked(void* dst, const void* src, size_t bytes, cudaMemcpyKin
   return cudaSuccess;
 }
 
+// The copies of a large request are fed to the copy engines a few 8 MiB
+// pieces at a time (a "pump"), so that a small request's copy queued
+// meanwhile waits for at most kPumpDepth pieces, not for the whole transfer.
+// Large requests also take each direction in turn, in admission order.
+// States: 0 waits for the host-to-device lane, 1 issues its pieces, 2 waits
+// for the device-to-host lane (the transform is issued), 3 issues those
+// pieces, 4 done (the request's completion event is recorded).
+constexpr int kPumpDepth = 2;
+constexpr std::chrono::microseconds kPumpHold(2000);
+struct Pump {
+  std::shared_ptr<Request> r;
+  cudaStream_t st = nullptr;
+  int si = 0;
+  int state = 0;
+  size_t off = 0;
+  cudaEvent_t ev[kPumpDepth] = {};
+  int head = 0, count = 0;
+  bool holding = false;  // a piece held back for small copies since hold_since
+  Clock::time_point hold_since;
+};
+
+// Drop the finished copies at the front of `q`; true while one is pending.
+bool copies_pending(std::deque<cudaEvent_t>& q) {
+  while (!q.empty()) {
+    const cudaError_t e = cudaEventQuery(q.front());
+    if (e == cudaErrorNotReady) return true;
+    cudaEventDestroy(q.front());  // done (or failed: its request reports that)
+    q.pop_front();
+  }
+  return false;
+}
+
+// Advance one pump as far as it can go now; `lane_h2d` / `lane_d2h` say
+// whether an earlier pump holds that lane.  Returns a CUDA error, or
+// cudaSuccess (also when it had to wait).
+cudaError_t pump_step(shafft_sm100_server_s* s, Pump& p, bool lane_h2d, bool lane_d2h) {
+  Request& r = *p.r;
+  while (p.count > 0) {  // retire finished pieces
+    const cudaError_t q = cudaEventQuery(p.ev[p.head]);
+    if (q == cudaErrorNotReady) break;
+    if (q != cudaSuccess) return q;
+    p.head = (p.head + 1) % kPumpDepth;
+    p.count--;
+  }
+  cudaError_t e = cudaSuccess;
+  for (;;) {
+    if (p.state == 0) {
+      if (lane_h2d) return cudaSuccess;
+      e = cudaStreamWaitEvent(p.st, s->large_h2d, 0);
+      if (e != cudaSuccess) return e;
+      p.state = 1;
+      p.off = 0;
+    } else if (p.state == 2) {
+      if (lane_d2h) return cudaSuccess;
+      e = cudaStreamWaitEvent(p.st, s->large_d2h, 0);
+      if (e != cudaSuccess) return e;
+      p.state = 3;
+      p.off = 0;
+    } else if (p.state == 1 || p.state == 3) {
+      if (p.off < r.bytes) {
+        if (p.count == kPumpDepth) return cudaSuccess;  // wait for a piece to finish
+        // hold the piece back for pending small copies, for at most
+        // kPumpHold at a stretch so that a steady stream of small requests
+        // cannot starve the large one
+        if (copies_pending(p.state == 1 ? s->small_h2d : s->small_d2h)) {
+          const auto now = Clock::now();
+          if (!p.holding) {
+            p.holding = true;
+            p.hold_since = now;
+          }
+          if (now - p.hold_since < kPumpHold) return cudaSuccess;
+        }
+        p.holding = false;
+        const size_t n = std::min(kCopyChunk, r.bytes - p.off);
+        e = p.state == 1 ? cudaMemcpyAsync(static_cast<char*>(r.d_in) + p.off,
+                                           static_cast<const char*>(r.host_in) + p.off, n,
+                                           cudaMemcpyHostToDevice, p.st)
+                         : cudaMemcpyAsync(static_cast<char*>(r.host_out) + p.off,
+                                           static_cast<const char*>(r.d_out) + p.off, n,
+                                           cudaMemcpyDeviceToHost, p.st);
+        if (e == cudaSuccess) e = cudaEventRecord(p.ev[(p.head + p.count) % kPumpDepth], p.st);
+        if (e != cudaSuccess) return e;
+        p.count++;
+        p.off += n;
+      } else if (p.state == 1) {
+        e = cudaEventRecord(s->large_h2d, p.st);
+        if (e != cudaSuccess) return e;
+        const int xrc = shafft_sm100_execute(r.inst->plan, r.d_in, r.d_out, r.direction, r.scale, p.st);
+        if (xrc) {
+          r.status = xrc;  // the library's own status; the caller reports it
+          return cudaErrorUnknown;
+        }
+        p.state = 2;
+      } else {
+        e = cudaEventRecord(s->large_d2h, p.st);
+        if (e == cudaSuccess) e = cudaFreeAsync(r.d_in, p.st);
+        if (e == cudaSuccess) r.d_in = nullptr;
+        if (e == cudaSuccess) e = cudaFreeAsync(r.d_out, p.st);
+        if (e == cudaSuccess) r.d_out = nullptr;
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(r.ev, p.st);
+        if (e != cudaSuccess) return e;
+        p.state = 4;
+        return cudaSuccess;
+      }
+    } else {
+      return cudaSuccess;
+    }
+  }
+}
+
+// caller holds s->mu: a request that failed while being issued
+void fail_issue(shafft_sm100_server_s* s, Request& r, cudaError_t e) {
+  if (!r.status) r.status = sfail(SHAFFT_SM100_ECUDA, "issue: %s", cudaGetErrorString(e));
+  cudaStreamSynchronize(s->streams[r.stream]);
+  r.done = true;
+  r.t_done = Clock::now();
+  s->used -= 2 * r.bytes;
+  s->stream_bytes[r.stream] -= 2 * r.bytes;
+  r.inst->users--;
+  s->failed++;
+  s->cv_done.notify_all();
+}
+
 void dispatcher_loop(shafft_sm100_server_s* s) {
   cudaSetDevice(s->device);
+  std::vector<Pump> pumps;  // large requests whose copies are being fed
   std::unique_lock<std::mutex> lk(s->mu);
-  while (!s->stop) {
+  while (!s->stop || !pumps.empty()) {
+    if (!pumps.empty()) {
+      const auto t0 = Clock::now();
+      lk.unlock();
+      // in admission order: a pump waits for a lane held or awaited by an earlier one
+      bool h2d_busy = false, d2h_busy = false;
+      std::vector<cudaError_t> errs(pumps.size(), cudaSuccess);
+      for (size_t i = 0; i < pumps.size(); ++i) {
+        errs[i] = pump_step(s, pumps[i], h2d_busy, d2h_busy);
+        const int st = pumps[i].state;
+        h2d_busy |= (st <= 1);
+        d2h_busy |= (st == 2 || st == 3);
+      }
+      lk.lock();
+      s->issue_ms_max = std::max(s->issue_ms_max, std::chrono::duration<double, std::milli>(Clock::now() - t0).count());
+      for (size_t i = pumps.size(); i-- > 0;) {
+        Pump& p = pumps[i];
+        if (errs[i] == cudaSuccess && p.state != 4) continue;
+        if (errs[i] != cudaSuccess) {
+          if (p.r->d_in) cudaFreeAsync(p.r->d_in, p.st);
+          if (p.r->d_out) cudaFreeAsync(p.r->d_out, p.st);
+          fail_issue(s, *p.r, errs[i]);
+        } else {
+          s->inflight.push_back(p.r);
+          s->max_inflight_seen = std::max<int>(s->max_inflight_seen, (int)s->inflight.size());
+        }
+        for (cudaEvent_t ev : p.ev)
+          if (ev) cudaEventDestroy(ev);
+        pumps.erase(pumps.begin() + i);
+      }
+    }
+    const auto nap = pumps.empty() ? std::chrono::microseconds(20000) : std::chrono::microseconds(50);
+    if (s->stop) {
+      s->cv_queue.wait_for(lk, nap);
+      continue;
+    }
     if (s->queue.empty()) {
-      s->cv_queue.wait_for(lk, std::chrono::milliseconds(20));
+      s->cv_queue.wait_for(lk, nap);
       continue;
     }
     {
@@ -284,7 +467,7 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
           continue;  // the queue may have changed meanwhile
         }
       }
-      if (s->used + hneed > s->budget && s->inflight.empty() && s->building.empty()) {
+      if (s->used + hneed > s->budget && s->inflight.empty() && pumps.empty() && s->building.empty()) {
         // can never fit: fail it instead of blocking the queue
         s->queue.pop_front();
         head->status = sfail(SHAFFT_SM100_EALLOC, "request needs %zu bytes, budget %zu", hneed, s->budget);
@@ -310,53 +493,87 @@ void dispatcher_loop(shafft_sm100_server_s* s) {
       }
     }
     if (!r) {
-      s->cv_queue.wait_for(lk, std::chrono::microseconds(200));
+      s->cv_queue.wait_for(lk, pumps.empty() ? std::chrono::microseconds(200) : std::chrono::microseconds(50));
       continue;
     }
     const size_t need = 2 * r->bytes;
     s->used += need;
-    // least recently used stream
+    // the stream with the fewest bytes of requests still in flight (the
+    // least recently used among equals): a request issued behind a large
+    // one on the same stream would wait for all of it
     int si = 0;
     for (int i = 1; i < s->nstreams; ++i)
-      if (s->stream_last[i] < s->stream_last[si]) si = i;
+      if (s->stream_bytes[i] < s->stream_bytes[si] ||
+          (s->stream_bytes[i] == s->stream_bytes[si] && s->stream_last[i] < s->stream_last[si]))
+        si = i;
     s->stream_last[si] = Clock::now();
+    s->stream_bytes[si] += need;
     r->inst = inst;
     r->stream = si;
     cudaStream_t st = s->streams[si];
+    const auto t_issue = Clock::now();
+    r->t_issue = t_issue;
     lk.unlock();
     cudaError_t e = cudaMallocFromPoolAsync(&r->d_in, r->bytes, s->pool, st);
     if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&r->d_out, r->bytes, s->pool, st);
+    if (e == cudaSuccess && r->bytes >= kLargeCopy) {
+      // a large request: its copies go through a pump
+      Pump p;
+      p.r = r;
+      p.st = st;
+      p.si = si;
+      for (int k = 0; k < kPumpDepth && e == cudaSuccess; ++k)
+        e = cudaEventCreateWithFlags(&p.ev[k], cudaEventDisableTiming);
+      if (e == cudaSuccess) {
+        lk.lock();
+        s->issue_ms_max =
+            std::max(s->issue_ms_max, std::chrono::duration<double, std::milli>(Clock::now() - t_issue).count());
+        pumps.push_back(p);
+        continue;
+      }
+      for (cudaEvent_t ev : p.ev)
+        if (ev) cudaEventDestroy(ev);
+    }
+    // a copy that a pump should let through first: an event after it
+    auto mark = [&](std::deque<cudaEvent_t>& q) {
+      if (pumps.empty() || e != cudaSuccess) return;
+      cudaEvent_t ev = nullptr;
+      e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventRecord(ev, st);
+      if (e == cudaSuccess)
+        q.push_back(ev);
+      else if (ev)
+        cudaEventDestroy(ev);
+    };
     if (e == cudaSuccess) e = copy_chunked(r->d_in, r->host_in, r->bytes, cudaMemcpyHostToDevice, st);
+    mark(s->small_h2d);
     int xrc = 0;
     if (e == cudaSuccess)
       xrc = shafft_sm100_execute(inst->plan, r->d_in, r->d_out, r->direction, r->scale, st);
     if (e == cudaSuccess && !xrc)
       e = copy_chunked(r->host_out, r->d_out, r->bytes, cudaMemcpyDeviceToHost, st);
+    if (!xrc) mark(s->small_d2h);
     if (r->d_in) cudaFreeAsync(r->d_in, st);
     if (r->d_out) cudaFreeAsync(r->d_out, st);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventRecord(r->ev, st);
     lk.lock();
+    s->issue_ms_max = std::max(s->issue_ms_max, std::chrono::duration<double, std::milli>(Clock::now() - t_issue).count());
     if (e != cudaSuccess || xrc) {
-      r->status = xrc ? xrc : sfail(SHAFFT_SM100_ECUDA, "issue: %s", cudaGetErrorString(e));
-      cudaStreamSynchronize(st);
-      r->done = true;
-      r->t_done = Clock::now();
-      s->used -= need;
-      inst->users--;
-      s->failed++;
-      s->cv_done.notify_all();
+      if (xrc) r->status = xrc;
+      fail_issue(s, *r, e);
       continue;
     }
     s->inflight.push_back(r);
     s->max_inflight_seen = std::max<int>(s->max_inflight_seen, (int)s->inflight.size());
   }
+  s->dispatch_done = true;
 }
 
 void completer_loop(shafft_sm100_server_s* s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
-  while (!s->stop || !s->inflight.empty()) {
+  while (!s->dispatch_done || !s->inflight.empty()) {
     bool any = false;
     for (size_t i = 0; i < s->inflight.size();) {
       auto r = s->inflight[i];
@@ -372,6 +589,7 @@ void completer_loop(shafft_sm100_server_s* s) {
         s->failed++;
       } else {
         s->completed++;
+        s->admit_ms.push_back(std::chrono::duration<double, std::milli>(r->t_issue - r->t_submit).count());
         s->latencies_ms.push_back(
             std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
         if (s->completed == 1) s->t_first = r->t_submit;
@@ -380,6 +598,7 @@ void completer_loop(shafft_sm100_server_s* s) {
       cudaEventDestroy(r->ev);
       r->ev = nullptr;
       s->used -= 2 * r->bytes;
+      s->stream_bytes[r->stream] -= 2 * r->bytes;
       r->inst->users--;
       r->inst->last_used = Clock::now();
       r->done = true;
@@ -430,16 +649,21 @@ int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, in
     int no = 0;
     e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
   }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->large_h2d, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->large_d2h, cudaEventDisableTiming);
   for (int i = 0; e == cudaSuccess && i < streams; ++i) {
     cudaStream_t st = nullptr;
     e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     s->streams.push_back(st);
     s->stream_last.push_back(Clock::now());
+    s->stream_bytes.push_back(0);
   }
   if (e != cudaSuccess) {
     for (auto st : s->streams)
       if (st) cudaStreamDestroy(st);
     if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->large_h2d) cudaEventDestroy(s->large_h2d);
+    if (s->large_d2h) cudaEventDestroy(s->large_d2h);
     delete s;
     return sfail(SHAFFT_SM100_ECUDA, "server set-up: %s", cudaGetErrorString(e));
   }
@@ -510,7 +734,9 @@ int shafft_sm100_server_wait(shafft_sm100_server s, uint64_t id, double* latency
 int shafft_sm100_server_stats(shafft_sm100_server s, char* buf, int buflen) {
   if (!s || !buf || buflen <= 0) return sfail(SHAFFT_SM100_EINVAL, "bad arguments");
   std::lock_guard<std::mutex> lk(s->mu);
-  std::vector<double> v = s->latencies_ms;
+  std::vector<double> v = s->latencies_ms, va = s->admit_ms;
+  std::sort(va.begin(), va.end());
+  const double admit_p99 = va.empty() ? 0.0 : va[std::min(va.size() - 1, (size_t)(0.99 * (va.size() - 1) + 0.5))];
   std::sort(v.begin(), v.end());
   auto pct = [&](double q) { return v.empty() ? 0.0 : v[std::min(v.size() - 1, (size_t)(q * (v.size() - 1) + 0.5))]; };
   const double span = s->completed ? std::chrono::duration<double>(s->t_last - s->t_first).count() : 0;
@@ -518,11 +744,11 @@ int shafft_sm100_server_stats(shafft_sm100_server s, char* buf, int buflen) {
            "{\"completed\":%llu,\"failed\":%llu,\"p50_ms\":%.4f,\"p99_ms\":%.4f,\"max_ms\":%.4f,"
            "\"throughput_per_s\":%.3f,\"max_inflight\":%d,\"resident_plan_bytes\":%zu,\"streams\":%d,"
            "\"plans_created\":%llu,\"plans_evicted\":%llu,\"plan_create_ms_total\":%.3f,"
-           "\"plan_create_ms_max\":%.3f}",
+           "\"plan_create_ms_max\":%.3f,\"issue_ms_max\":%.3f,\"admit_wait_p99_ms\":%.4f}",
            (unsigned long long)s->completed, (unsigned long long)s->failed, pct(0.5), pct(0.99),
            v.empty() ? 0.0 : v.back(), span > 0 ? s->completed / span : 0.0, s->max_inflight_seen,
            s->plan_bytes, s->nstreams, (unsigned long long)s->plans_created,
-           (unsigned long long)s->plans_evicted, s->create_ms_total, s->create_ms_max);
+           (unsigned long long)s->plans_evicted, s->create_ms_total, s->create_ms_max, s->issue_ms_max, admit_p99);
   return 0;
 }
 
@@ -530,10 +756,12 @@ int shafft_sm100_server_reset_stats(shafft_sm100_server s) {
   if (!s) return sfail(SHAFFT_SM100_EINVAL, "null server");
   std::lock_guard<std::mutex> lk(s->mu);
   s->latencies_ms.clear();
+  s->admit_ms.clear();
   s->completed = s->failed = 0;
   s->max_inflight_seen = 0;
   s->plans_created = s->plans_evicted = 0;
   s->create_ms_total = s->create_ms_max = 0;
+  s->issue_ms_max = 0;
   return 0;
 }
 
@@ -555,6 +783,10 @@ int shafft_sm100_server_destroy(shafft_sm100_server s) {
   for (auto& kv : s->plans)
     for (auto& p : kv.second) shafft_sm100_plan_destroy(p->plan);
   if (s->pool) cudaMemPoolDestroy(s->pool);
+  cudaEventDestroy(s->large_h2d);
+  cudaEventDestroy(s->large_d2h);
+  for (auto* q : {&s->small_h2d, &s->small_d2h})
+    for (cudaEvent_t ev : *q) cudaEventDestroy(ev);
   delete s;
   return 0;
 }
