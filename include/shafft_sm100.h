@@ -215,15 +215,21 @@ int shafft_sm100_batch_describe(shafft_sm100_batch b, char* buf, int buflen);
  * buffers -- pinned for overlap) are admitted in arrival order as soon as
  * their two device buffers fit `budget_bytes` (resident plans count against
  * the budget; idle plans are evicted oldest first, and only when the
- * resident plans alone leave no room), issued on the least recently used
- * of the streams (H2D, execute, D2H, in pieces of at most 8 MiB) and so
- * overlap with requests already running.  Creation grows the device memory
- * pool to the budget (or to what the device can spare), so request buffers
- * are carved out of memory mapped up front.
+ * resident plans alone leave no room), issued on the stream with the
+ * fewest bytes in flight (H2D, execute, D2H, in pieces of at most 8 MiB)
+ * and so overlap with requests already running.  Requests with buffers of
+ * 256 MiB or more copy one per direction at a time, fed to the copy engines
+ * two pieces at a time and held back (at most 2 ms a piece) while smaller
+ * requests' copies are pending, so a small request does not wait behind a
+ * large transfer.  Requests of one shape share a plan instance when the plan
+ * has no scratch.  The server's own memory pool is grown to the budget (or
+ * to what the device can spare) at creation, so request buffers are carved
+ * out of memory mapped up front.
  * wait() blocks until the request's output is in host_out and returns its
  * status and latency (submission to completion).  stats() reports completed
- * / failed counts, p50 / p99 / max latency, throughput and plan-instance
- * creations / evictions as JSON.  Wait for every submitted request before
+ * / failed counts, p50 / p99 / max latency, throughput, plan-instance
+ * creations / evictions, the longest issue step and the p99 wait from
+ * submission to issue as JSON.  Wait for every submitted request before
  * destroy. */
 typedef struct shafft_sm100_server_s* shafft_sm100_server;
 int shafft_sm100_server_create(shafft_sm100_server* out, size_t budget_bytes, int streams);
