@@ -127,3 +127,56 @@ def test_tight_budget_alternating_shapes_evicts_and_completes():
     assert st["failed"] == 0 and st["completed"] == 6
     assert st["plans_evicted"] >= 1
     srv.destroy()
+
+
+def test_large_requests_through_the_copy_pump():
+    """Requests with buffers of 256 MiB or more go through the copy pump
+    (pieces fed a few at a time, one large request per direction at a time,
+    held back while smaller copies are pending).  Two of them overlapping
+    each other and a stream of small requests: every result is bit-identical
+    to the same request served alone, and the large ones match a plain plan
+    execute."""
+    shape = (256, 512, 256)  # 256 MiB of complex64
+    n = math.prod(shape)
+    srv = _sm100.Server(budget_bytes=8 << 30, streams=4)
+    bigs = []
+    for i in range(2):
+        g = torch.Generator().manual_seed(100 + i)
+        x = (torch.rand(2 * n, generator=g) * 2 - 1).view(torch.complex64).pin_memory()
+        bigs.append((x, torch.empty_like(x).pin_memory(), i % 2))
+    smalls = []
+    for i in range(12):
+        x = o.uniform_input((64, 128), seed=200 + i, dtype=np.complex64)
+        smalls.append((pinned(x), pinned(np.zeros_like(x)), pinned(np.zeros_like(x))))
+    # alone
+    alone_big = []
+    for x, out, d in bigs:
+        rid = srv.submit(shape, 0, d, 1.0, x.data_ptr(), out.data_ptr())
+        srv.wait(rid)
+        alone_big.append(out.clone())
+    for a, out_alone, _ in smalls:
+        srv.wait(srv.submit((64, 128), 0, 0, 1.0, a.data_ptr(), out_alone.data_ptr()))
+    # mixed: both large ones, small ones between them
+    ids = [srv.submit(shape, 0, bigs[0][2], 1.0, bigs[0][0].data_ptr(), bigs[0][1].data_ptr())]
+    for a, _, out_mix in smalls[:6]:
+        ids.append(srv.submit((64, 128), 0, 0, 1.0, a.data_ptr(), out_mix.data_ptr()))
+    ids.append(srv.submit(shape, 0, bigs[1][2], 1.0, bigs[1][0].data_ptr(), bigs[1][1].data_ptr()))
+    for a, _, out_mix in smalls[6:]:
+        ids.append(srv.submit((64, 128), 0, 0, 1.0, a.data_ptr(), out_mix.data_ptr()))
+    for rid in ids:
+        srv.wait(rid)
+    for (x, out, d), ref in zip(bigs, alone_big):
+        assert torch.equal(out, ref)
+    for _, out_alone, out_mix in smalls:
+        np.testing.assert_array_equal(out_mix.numpy(), out_alone.numpy())
+    assert srv.stats()["failed"] == 0
+    srv.destroy()
+    # the large results against a plain plan on the device
+    plan = _sm100.Plan(shape, 0)
+    for (x, _, d), ref in zip(bigs, alone_big):
+        a = x.cuda()
+        b = torch.empty_like(a)
+        plan.execute(a.data_ptr(), b.data_ptr(), d, 1.0, 0)
+        torch.cuda.synchronize()
+        assert torch.equal(b.cpu(), ref)
+    plan.destroy()
