@@ -313,6 +313,8 @@ def kernel_name(st):
     if st.get("fast"):
         if not st.get("in_row") and st.get("L") in (256, 512) and os.environ.get("SHAFFT_SM100_TMA", "0") != "0":
             return "k_fft_fast_tma"  # column tile fed by bulk tensor copies (when its view qualifies)
+        if st.get("prefetch") and not st.get("bs") and not st.get("map"):
+            return f"k_fft_fast_pf<IN_ROW={st.get('in_row', 0)}>"  # with the L2 prefetch of a later tile
         return f"k_fft_fast<IN_ROW={st.get('in_row', 0)}>"
     if st["kind"] == "plane":
         return "k_fft_plane_cluster" if st.get("cluster") else "k_fft_plane_flow"

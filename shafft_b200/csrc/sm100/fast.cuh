@@ -473,6 +473,52 @@ __global__ void __launch_bounds__(NT)
       g, in, out, tb, blockIdx.x, reinterpret_cast<float4*>(smem_raw));
 }
 
+// Ask L2 for every input line of tile `tile` (one prefetch per 128-byte
+// line; the same lines the tile's loads read, so only valid tiles).
+template <typename T, int L, int NT, bool IN_ROW>
+__device__ __forceinline__ void fast_prefetch(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile) {
+  using C = typename Cx<T>::type;
+  constexpr int W = 8 * ChunkT<T>::VW;
+  constexpr int LINE = 128 / (int)sizeof(C);
+  const int64_t bin = fast_tile_at<W>(g, tile).bin;
+  if constexpr (IN_ROW) {
+    constexpr int LPR = L / LINE;  // lines per input row
+    static_assert(LPR >= 1, "a row tile covers whole lines");
+    for (int l = threadIdx.x; l < W * LPR; l += NT)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(in + bin + (int64_t)(l / LPR) * g.sin[0] + (l % LPR) * LINE));
+  } else {
+    for (int l = threadIdx.x; l < L; l += NT)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(in + bin + (int64_t)l * g.sn_in));
+  }
+}
+
+// k_fft_fast with an L2 prefetch of the tile `ahead` tiles on (about one
+// wave of resident CTAs later), issued just before this tile's own loads
+// (so that no loaded data is live meanwhile); the prefetches hold no registers, so the SM has more reads in
+// flight than three tiles' worth of loads alone.  Same arithmetic and
+// results as k_fft_fast.
+// (Resident CTAs per SM it is compiled for: the occupancy the plain kernel
+// reaches at its own register count, so that the prefetch costs no CTA slot;
+// 80 registers for the complex64 512-point pass.)
+template <typename T, int L>
+constexpr int fast_pf_min_blocks() {
+  return sizeof(T) == 4 ? (L <= 256 ? 4 : (L == 512 ? 3 : 1)) : (L <= 256 ? 5 : 2);
+}
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW>
+__global__ void __launch_bounds__(NT, fast_pf_min_blocks<T, L>())
+    k_fft_fast_pf(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
+                  typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb,
+                  int64_t ahead) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float4* sm = reinterpret_cast<float4*>(smem_raw);
+  const int64_t nt = (int64_t)blockIdx.x + ahead;
+  if (nt < g.ntiles) fast_prefetch<T, L, NT, IN_ROW>(g, in, nt);
+  FastRegs<T, L, R0, R1, R2, NT> R;
+  fast_load<T, L, R0, R1, R2, NT, IN_ROW>(g, in, blockIdx.x, sm, LD_STREAM, R);
+  fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false>(g, in, out, tb, blockIdx.x, sm, R,
+                                                                         TilePolicy{0, 0, 0});
+}
+
 // Two axes of a stack of square L x L planes in one HBM pass, as a
 // persistent dataflow kernel.  Control words (zeroed before each launch):
 // 64-bit ticket counter at ctl[0..1], error flag ctl[2], per-plane counters

@@ -91,6 +91,10 @@ struct Launch {
                           const PassTables<C>& tb, int* err, cudaStream_t s);
   static bool fast_supported(int L);
   static int fast_threads(int L);
+  // L2 prefetch distance (quarter waves of resident CTAs) of the plain
+  // specialised pass of length L with row (in_row) or column input; 0 when
+  // it runs k_fft_fast without prefetching
+  static int fast_prefetch(int L, bool in_row);
   // fused two-axis pass over a stack of square L x L planes (see
   // k_fft_plane_flow); ctl holds 4 + planes ints of plan-owned device memory
   static cudaError_t plane(const PassGeom& gx, const PassGeom& gy, const C* src, C* mid, C* dst,
@@ -116,6 +120,10 @@ template <>
 int Launch<float>::fast_threads(int L);
 template <>
 int Launch<double>::fast_threads(int L);
+template <>
+int Launch<float>::fast_prefetch(int L, bool in_row);
+template <>
+int Launch<double>::fast_prefetch(int L, bool in_row);
 template <>
 bool Launch<float>::plane_supported(int L);
 template <>

@@ -256,6 +256,63 @@ struct FastExt<float, L, A, B, C_, NT> {
   }
 };
 
+// L2 prefetch distance of k_fft_fast_pf, in quarter waves of resident CTAs
+// (0 runs k_fft_fast).  Row-input (transposing) passes:
+// SHAFFT_SM100_PREFETCH_ROW, default 4 (one wave); column-input passes:
+// SHAFFT_SM100_PREFETCH_COL, default 0.  Only the complex64 512-point pass
+// has a prefetching instantiation.  Measured on B200 (512^3 complex64
+// fwd+bwd): one wave ahead on the row passes takes them from 0.433 to
+// 0.39-0.40 ms each with per-launch timing and 2.56-2.62 -> 2.55-2.61 ms per
+// step under graph replay; half a wave, 1.5 waves and 2 waves were slower
+// than none (2.65-3.01 ms), prefetching the column pass slowed it (0.467 ->
+// 0.502 ms), and the same kernel at L = 256 (256^3 complex128 and
+// complex64, 2^24 complex64) lost 3-8%.
+static int prefetch_quarters(bool in_row) {
+  static const int v[2] = {[] {
+                             const char* e = getenv("SHAFFT_SM100_PREFETCH_COL");
+                             const int x = e ? atoi(e) : 0;
+                             return (x >= 0 && x <= 32) ? x : 0;
+                           }(),
+                           [] {
+                             const char* e = getenv("SHAFFT_SM100_PREFETCH_ROW");
+                             const int x = e ? atoi(e) : 4;
+                             return (x >= 0 && x <= 32) ? x : 4;
+                           }()};
+  return v[in_row ? 1 : 0];
+}
+
+template <typename T, int L, int A, int B, int C_, int NT>
+struct FastPf {
+  static constexpr bool kOn = sizeof(T) == 4 && L == 512;
+  static cudaError_t attr() {
+    if constexpr (kOn) {
+      cudaError_t e = cudaFuncSetAttribute(k_fft_fast_pf<T, L, A, B, C_, NT, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_fast_pf<T, L, A, B, C_, NT, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+      return e;
+    }
+    return cudaSuccess;
+  }
+  // false: not taken (switched off, or no prefetching instantiation for L)
+  static bool launch(bool in_row, unsigned grid, const PassGeom& g, const typename Vec2<T>::type* in,
+                     typename Vec2<T>::type* out, const PassTables<typename Vec2<T>::type>& tb, cudaStream_t s) {
+    if constexpr (kOn) {
+      const int q = prefetch_quarters(in_row);
+      if (q == 0) return false;
+      static const unsigned resident = resident_ctas(k_fft_fast_pf<T, L, A, B, C_, NT, true>, NT, L * 128);
+      const int64_t ahead = std::max<int64_t>(1, (int64_t)resident * q / 4);
+      if (in_row)
+        k_fft_fast_pf<T, L, A, B, C_, NT, true><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
+      else
+        k_fft_fast_pf<T, L, A, B, C_, NT, false><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
+      return true;
+    }
+    return false;
+  }
+};
+
 #define SHAFFT_DEFINE_PRECISION(TYPE, FASTLIST, PLANELIST)                                       \
   template <>                                                                                    \
   cudaError_t fast_attr_all<TYPE>() {                                                            \
@@ -276,6 +333,13 @@ struct FastExt<float, L, A, B, C_, NT> {
   int Launch<TYPE>::fast_threads(int L) {                                                        \
     switch (L) {                                                                                 \
       FASTLIST(SHAFFT_CASE_NT)                                                                   \
+      default: return 0;                                                                         \
+    }                                                                                            \
+  }                                                                                              \
+  template <>                                                                                    \
+  int Launch<TYPE>::fast_prefetch(int L, bool in_row) {                                          \
+    switch (L) {                                                                                 \
+      FASTLIST(SHAFFT_CASE_PF)                                                                   \
       default: return 0;                                                                         \
     }                                                                                            \
   }                                                                                              \
@@ -323,7 +387,8 @@ static cudaError_t fast_attr_all();
   if (e == cudaSuccess)                                                                           \
     e = cudaFuncSetAttribute(k_fft_fast<TYPE_, L, A, B, C_, NT, false>,                           \
                              cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);               \
-  if (e == cudaSuccess) e = FastExt<TYPE_, L, A, B, C_, NT>::attr();
+  if (e == cudaSuccess) e = FastExt<TYPE_, L, A, B, C_, NT>::attr();                             \
+  if (e == cudaSuccess) e = FastPf<TYPE_, L, A, B, C_, NT>::attr();
 #define SHAFFT_ATTR_PLANE(L, A, B, C_, NT)                                                        \
   if (e == cudaSuccess)                                                                           \
     e = cudaFuncSetAttribute(k_fft_plane_flow<TYPE_, L, A, B, C_, NT>,                            \
@@ -352,12 +417,16 @@ static cudaError_t fast_attr_all();
 #define SHAFFT_CASE_TRUE(L_, A, B, C_, NT) \
   case L_:                                 \
     return true;
+#define SHAFFT_CASE_PF(L_, A, B, C_, NT) \
+  case L_:                               \
+    return FastPf<TYPE_, L_, A, B, C_, NT>::kOn ? prefetch_quarters(in_row) : 0;
 #define SHAFFT_CASE_NT(L_, A, B, C_, NT) \
   case L_:                               \
     return NT;
 #define SHAFFT_CASE_FAST(L_, A, B, C_, NT)                                                       \
   case L_:                                                                                       \
     if (g.bs_mode || g.map_mode) return FastExt<TYPE_, L_, A, B, C_, NT>::launch(in_row, grid, g, in, out, tb, s); \
+    if (FastPf<TYPE_, L_, A, B, C_, NT>::launch(in_row, grid, g, in, out, tb, s)) return cudaGetLastError(); \
     if (in_row)                                                                                  \
       k_fft_fast<TYPE_, L_, A, B, C_, NT, true><<<grid, NT, L_ * 128, s>>>(g, in, out, tb);      \
     else                                                                                         \

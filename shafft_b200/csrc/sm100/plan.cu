@@ -1282,6 +1282,14 @@ struct Launcher {
   }
 };
 
+// L2 prefetch distance a pass step launches with (Launch<T>::fast_prefetch):
+// plain specialised passes only
+static int pass_prefetch(int precision, const Step& st) {
+  if (!st.fast || st.tc || st.g.bs_mode || st.g.map_mode) return 0;
+  return precision ? Launch<double>::fast_prefetch(st.g.L, st.g.in_row != 0)
+                   : Launch<float>::fast_prefetch(st.g.L, st.g.in_row != 0);
+}
+
 std::string describe_steps(int precision, const std::vector<Step>& steps, int64_t total) {
   std::string s = "{\"precision\":" + std::to_string(precision) + ",\"elements\":" +
                   std::to_string(total) + ",\"steps\":[";
@@ -1304,11 +1312,12 @@ std::string describe_steps(int precision, const std::vector<Step>& steps, int64_
                "{\"kind\":\"pass\",\"L\":%d,\"radices\":[%s],\"W\":%d,\"in\":\"%s\",\"out\":\"%s\","
                "\"in_row\":%d,\"out_row\":%d,\"tiles\":%lld,\"smem\":%zu,\"twiddle\":%d,"
                "\"ext\":[%lld,%lld,%lld,%lld],\"sn_in\":%lld,\"sk_out\":%lld,\"fast\":%d,\"tc\":%d,\"bs\":%d,"
-               "\"map\":%d}",
+               "\"map\":%d,\"prefetch\":%d}",
                st.g.L, rad.c_str(), st.g.W, buf_name(st.in_buf), buf_name(st.out_buf), st.g.in_row,
                st.g.out_row, (long long)st.g.ntiles, st.smem, st.g.tw_mode, (long long)st.g.ext[0],
                (long long)st.g.ext[1], (long long)st.g.ext[2], (long long)st.g.ext[3],
-               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast, st.tc, st.g.bs_mode, st.g.map_mode);
+               (long long)st.g.sn_in, (long long)st.g.sk_out, st.fast, st.tc, st.g.bs_mode, st.g.map_mode,
+               pass_prefetch(precision, st));
     } else {
       const char* k = st.kind == ST_BS_MOD    ? "bluestein_modulate"
                       : st.kind == ST_BS_MULH ? "bluestein_multiply"

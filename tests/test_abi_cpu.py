@@ -2,8 +2,11 @@
 function include/*.h declares, and the host state machine returns the
 reference's status codes (src/cpp/shafft.cpp, src/cpp/shafft_internal.cpp)."""
 import ctypes
+import json
 import os
 import re
+import subprocess
+import sys
 import threading
 
 import pytest
@@ -225,6 +228,30 @@ def test_planner_pass_lists():
     for dims in ([63, 47, 31], [1 << 24], [4096, 3], [7, 11, 13, 17], [2, 3, 4, 5]):
         q = _sm100.plan_query(dims, 0)
         assert q["steps"][-1]["out"] == "dst", dims
+
+
+def test_planner_prefetch_passes():
+    """The complex64 512-point transposing passes run the prefetching kernel
+    (one wave ahead by default); column passes, other lengths and
+    complex128 run the plain kernel.  Run in a child process so that the
+    switches are read fresh."""
+    code = ("import json, sys; sys.path.insert(0, sys.argv[1]); from shafft_b200 import _sm100; "
+            "print(json.dumps([[s.get('prefetch') for s in _sm100.plan_query(d, p)['steps']] "
+            "for d, p in (([512, 512, 512], 0), ([512, 512, 512], 1), ([256, 256, 256], 0))]))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+    def query(**env):
+        e = {k: v for k, v in os.environ.items() if not k.startswith("SHAFFT_SM100_PREFETCH")}
+        e.update(env)
+        r = subprocess.run([sys.executable, "-c", code, root], env=e, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+    assert query() == [[4, 4, 0], [0, 0, 0], [0, 0, 0]]
+    assert query(SHAFFT_SM100_PREFETCH_ROW="0") == [[0, 0, 0], [0, 0, 0], [0, 0, 0]]
+    assert query(SHAFFT_SM100_PREFETCH_ROW="2", SHAFFT_SM100_PREFETCH_COL="3") == \
+        [[2, 2, 3], [0, 0, 0], [0, 0, 0]]
 
 
 def test_planner_balanced_splits():
