@@ -79,6 +79,15 @@ __device__ __forceinline__ float2 ld_stream<float2>(const float2* p) { return __
 template <>
 __device__ __forceinline__ double2 ld_stream<double2>(const double2* p) { return __ldcs(p); }
 __device__ __forceinline__ float4 ld_chunk(const void* p) { return __ldcs(reinterpret_cast<const float4*>(p)); }
+// The same load asking L2 to fetch the whole 256-byte block around the line
+// (the neighbouring column tile's line comes with it).
+__device__ __forceinline__ float4 ld_chunk_256(const void* p) {
+  float4 v;
+  asm volatile("ld.global.cs.L2::256B.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p));
+  return v;
+}
 __device__ __forceinline__ void st_chunk(void* p, float4 v) { __stcs(reinterpret_cast<float4*>(p), v); }
 template <typename C>
 __device__ __forceinline__ C ld_tw(const C* p) { return __ldg(p); }
@@ -165,14 +174,16 @@ __device__ __forceinline__ int64_t map_block(const PassGeom& g, int64_t v) {
 // Extended instantiations of the specialised pass (template argument EXT).
 enum FastExtKind : int { EXT_BS = 1, EXT_MAP = 2 };
 
-// Phase A loads: issue every input load of tile `tile` into R.
+// Phase A loads: issue every input load of tile `tile` into R (column
+// tiles with FETCH = 256: 256-byte L2 fetches).
 // EXT instantiations only: column tiles with PassGeom::bs_mode & BS_LOAD_MOD
 // read the Bluestein modulation of x on the fly (see pass.h; `chirp` is its
 // table), and map_mode & MAP_LOAD reads the input from an exchange's block
 // layout.  The plain instantiations carry none of this code: a runtime test
 // of bs_mode alone slowed the 512-point pass by a quarter; the two kinds are
 // separate instantiations so that each keeps its own register budget.
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false, int EXT = 0>
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, bool SMEM_A = false, int EXT = 0,
+          int FETCH = 0>
 __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile,
                                           const float4* sm, int LDP, FastRegs<T, L, R0, R1, R2, NT>& R,
                                           const typename Cx<T>::type* chirp = nullptr) {
@@ -220,7 +231,9 @@ __device__ __forceinline__ void fast_load(const PassGeom& g, const typename Cx<T
         int64_t off = bin + bc[b] * VW + (int64_t)n * g.sn_in;
         if ((EXT & EXT_MAP) && (g.map_mode & MAP_LOAD)) off = map_block(g, off);  // a chunk stays contiguous
         const void* src = in + off;
-        float4 raw = (LDP == LD_L2) ? __ldcg(reinterpret_cast<const float4*>(src)) : ld_chunk(src);
+        float4 raw = (LDP == LD_L2)  ? __ldcg(reinterpret_cast<const float4*>(src))
+                     : (FETCH == 256) ? ld_chunk_256(src)
+                                      : ld_chunk(src);
         const Chunk<C, VW> ch = *reinterpret_cast<const Chunk<C, VW>*>(&raw);
 #pragma unroll
         for (int e = 0; e < VW; ++e) R.v[b][r][e] = ch.v[e];
@@ -504,7 +517,9 @@ template <typename T, int L>
 constexpr int fast_pf_min_blocks() {
   return sizeof(T) == 4 ? (L <= 256 ? 4 : (L == 512 ? 3 : 1)) : (L <= 256 ? 5 : 2);
 }
-template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW>
+// FETCH = 256 (column tiles): the tile's own loads ask for 256-byte L2
+// fetches; ahead = 0: no prefetch.
+template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int FETCH = 0>
 __global__ void __launch_bounds__(NT, fast_pf_min_blocks<T, L>())
     k_fft_fast_pf(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
                   typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb,
@@ -512,9 +527,9 @@ __global__ void __launch_bounds__(NT, fast_pf_min_blocks<T, L>())
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float4* sm = reinterpret_cast<float4*>(smem_raw);
   const int64_t nt = (int64_t)blockIdx.x + ahead;
-  if (nt < g.ntiles) fast_prefetch<T, L, NT, IN_ROW>(g, in, nt);
+  if (ahead > 0 && nt < g.ntiles) fast_prefetch<T, L, NT, IN_ROW>(g, in, nt);
   FastRegs<T, L, R0, R1, R2, NT> R;
-  fast_load<T, L, R0, R1, R2, NT, IN_ROW>(g, in, blockIdx.x, sm, LD_STREAM, R);
+  fast_load<T, L, R0, R1, R2, NT, IN_ROW, false, 0, FETCH>(g, in, blockIdx.x, sm, LD_STREAM, R);
   fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false>(g, in, out, tb, blockIdx.x, sm, R,
                                                                          TilePolicy{0, 0, 0});
 }

@@ -281,6 +281,16 @@ static int prefetch_quarters(bool in_row) {
   return v[in_row ? 1 : 0];
 }
 
+// SHAFFT_SM100_COL_FETCH = 256 (default 0): the complex64 512-point passes
+// with column input load with 256-byte L2 fetches (k_fft_fast_pf<..., 256>).
+static bool col_fetch_256() {
+  static const bool on = [] {
+    const char* e = getenv("SHAFFT_SM100_COL_FETCH");
+    return e && atoi(e) == 256;
+  }();
+  return on;
+}
+
 template <typename T, int L, int A, int B, int C_, int NT>
 struct FastPf {
   static constexpr bool kOn = sizeof(T) == 4 && L == 512;
@@ -291,6 +301,9 @@ struct FastPf {
       if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_fft_fast_pf<T, L, A, B, C_, NT, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_fft_fast_pf<T, L, A, B, C_, NT, false, 256>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, L * 128);
       return e;
     }
     return cudaSuccess;
@@ -300,11 +313,14 @@ struct FastPf {
                      typename Vec2<T>::type* out, const PassTables<typename Vec2<T>::type>& tb, cudaStream_t s) {
     if constexpr (kOn) {
       const int q = prefetch_quarters(in_row);
-      if (q == 0) return false;
+      const bool fetch = !in_row && col_fetch_256();
+      if (q == 0 && !fetch) return false;
       static const unsigned resident = resident_ctas(k_fft_fast_pf<T, L, A, B, C_, NT, true>, NT, L * 128);
-      const int64_t ahead = std::max<int64_t>(1, (int64_t)resident * q / 4);
+      const int64_t ahead = q == 0 ? 0 : std::max<int64_t>(1, (int64_t)resident * q / 4);
       if (in_row)
         k_fft_fast_pf<T, L, A, B, C_, NT, true><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
+      else if (fetch)
+        k_fft_fast_pf<T, L, A, B, C_, NT, false, 256><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
       else
         k_fft_fast_pf<T, L, A, B, C_, NT, false><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
       return true;

@@ -3,8 +3,9 @@ tile (k_fft_fast_pf; on by default for row-input passes, one wave ahead)
 against the plain kernel (SHAFFT_SM100_PREFETCH_ROW=0): the prefetch only
 warms L2, the butterflies are the same, so the outputs must be
 bit-identical.  A third run also prefetches the column-input passes
-(SHAFFT_SM100_PREFETCH_COL=4).  The switches are read once per process, so
-each setting runs in a child process.  Every result is also checked against
+(SHAFFT_SM100_PREFETCH_COL=4); a fourth loads the column-input passes with
+256-byte L2 fetches instead (SHAFFT_SM100_COL_FETCH=256).  The switches are
+read once per process, so each setting runs in a child process.  Every result is also checked against
 the oracle (1e-6*log2(N)).  The shapes cover the transposing pair of a 3-D
 plan with few and many tiles (the prefetch target past the last tile is
 skipped), a row pass followed by other lengths, and the four-step twiddled
@@ -70,6 +71,7 @@ def test_prefetching_pass_matches_plain_pass_bitwise(tmp_path):
     on = _child(tmp_path, "on")
     off = _child(tmp_path, "off", SHAFFT_SM100_PREFETCH_ROW="0")
     col = _child(tmp_path, "col", SHAFFT_SM100_PREFETCH_COL="4")
+    fetch = _child(tmp_path, "fetch", SHAFFT_SM100_COL_FETCH="256")
     for i, dims in enumerate(CASES):
         # the default prefetches every 512-point row pass, and only those
         pf_on, pf_off, pf_col = (np.load(d / f"c{i}_pf.npy") for d in (on, off, col))
@@ -85,6 +87,8 @@ def test_prefetching_pass_matches_plain_pass_bitwise(tmp_path):
             y_col = np.load(col / f"c{i}_d{direction}.npy")
             assert np.array_equal(y_on.view(np.uint32), y_off.view(np.uint32)), (dims, direction)
             assert np.array_equal(y_col.view(np.uint32), y_off.view(np.uint32)), (dims, direction)
+            y_fetch = np.load(fetch / f"c{i}_d{direction}.npy")
+            assert np.array_equal(y_fetch.view(np.uint32), y_off.view(np.uint32)), (dims, direction)
             if direction == 0:
                 assert o.rel_l2(y_on, ref) <= tol, dims
             else:
