@@ -315,8 +315,14 @@ struct FastPf {
       const int q = prefetch_quarters(in_row);
       const bool fetch = !in_row && col_fetch_256();
       if (q == 0 && !fetch) return false;
-      static const unsigned resident = resident_ctas(k_fft_fast_pf<T, L, A, B, C_, NT, true>, NT, L * 128);
-      const int64_t ahead = q == 0 ? 0 : std::max<int64_t>(1, (int64_t)resident * q / 4);
+      // resident CTAs on the current device: its SMs x the CTAs per SM the
+      // kernel is compiled for (its 64 KiB tile fits that many)
+      int dev = 0, sms = 148;
+      if (cudaGetDevice(&dev) != cudaSuccess ||
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        sms = 148;
+      const int64_t resident = (int64_t)sms * fast_pf_min_blocks<T, L>();
+      const int64_t ahead = q == 0 ? 0 : std::max<int64_t>(1, resident * q / 4);
       if (in_row)
         k_fft_fast_pf<T, L, A, B, C_, NT, true><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
       else if (fetch)
