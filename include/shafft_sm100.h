@@ -175,7 +175,11 @@ int shafft_sm100_execute_step(shafft_sm100_plan plan, int step, void* src, void*
  * what the kernel touches), or 0 for an invalid step. */
 int64_t shafft_sm100_step_bytes(shafft_sm100_plan plan, int step);
 
-/* JSON description of a created plan. */
+/* JSON description of a created plan: its steps in order, each pass with
+ * its length, radices, tile width, buffers, row/column input and output,
+ * tile count, shared memory, twiddle mode, kernel kind (fast, tc, bs, map)
+ * and "prefetch", the L2 prefetch distance of the pass in quarter waves of
+ * resident CTAs (0 = none; see SHAFFT_SM100_PREFETCH_ROW). */
 int shafft_sm100_plan_describe(shafft_sm100_plan plan, char* buf, int buflen);
 
 /* ---- Batched form: many independent transforms in one launch ----------
