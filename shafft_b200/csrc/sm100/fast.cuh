@@ -487,9 +487,13 @@ __global__ void __launch_bounds__(NT)
 }
 
 // Ask L2 for every input line of tile `tile` (one prefetch per 128-byte
-// line; the same lines the tile's loads read, so only valid tiles).
+// line; the same lines the tile's loads read, so only valid tiles).  bulk
+// (row tiles): one bulk asynchronous prefetch per row (cp.async.bulk.
+// prefetch.L2, L points from a 16-byte aligned row start; rows that do not
+// start on 16 bytes take the per-line prefetches).
 template <typename T, int L, int NT, bool IN_ROW>
-__device__ __forceinline__ void fast_prefetch(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile) {
+__device__ __forceinline__ void fast_prefetch(const PassGeom& g, const typename Cx<T>::type* in, int64_t tile,
+                                              bool bulk) {
   using C = typename Cx<T>::type;
   constexpr int W = 8 * ChunkT<T>::VW;
   constexpr int LINE = 128 / (int)sizeof(C);
@@ -497,6 +501,20 @@ __device__ __forceinline__ void fast_prefetch(const PassGeom& g, const typename 
   if constexpr (IN_ROW) {
     constexpr int LPR = L / LINE;  // lines per input row
     static_assert(LPR >= 1, "a row tile covers whole lines");
+    static_assert((L * sizeof(C)) % 16 == 0, "a bulk prefetch moves whole 16-byte units");
+    if (bulk) {
+      static_assert(W <= NT, "one thread per row");
+      if (threadIdx.x < W) {
+        const C* row = in + bin + (int64_t)threadIdx.x * g.sin[0];
+        if ((reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(row), "r"((int)(L * sizeof(C)))
+                       : "memory");
+        } else {
+          for (int l = 0; l < LPR; ++l) asm volatile("prefetch.global.L2 [%0];" ::"l"(row + l * LINE));
+        }
+      }
+      return;
+    }
     for (int l = threadIdx.x; l < W * LPR; l += NT)
       asm volatile("prefetch.global.L2 [%0];" ::"l"(in + bin + (int64_t)(l / LPR) * g.sin[0] + (l % LPR) * LINE));
   } else {
@@ -506,10 +524,11 @@ __device__ __forceinline__ void fast_prefetch(const PassGeom& g, const typename 
 }
 
 // k_fft_fast with an L2 prefetch of the tile `ahead` tiles on (about one
-// wave of resident CTAs later), issued just before this tile's own loads
-// (so that no loaded data is live meanwhile); the prefetches hold no registers, so the SM has more reads in
-// flight than three tiles' worth of loads alone.  Same arithmetic and
-// results as k_fft_fast.
+// wave of resident CTAs later; row tiles by default as one bulk asynchronous
+// prefetch per row), issued just before this tile's own loads (so that no
+// loaded data is live meanwhile).  The prefetches hold no registers, so the
+// SM has more reads in flight than three tiles' worth of loads alone.  Same
+// arithmetic and results as k_fft_fast.
 // (Resident CTAs per SM it is compiled for: the occupancy the plain kernel
 // reaches at its own register count, so that the prefetch costs no CTA slot;
 // 80 registers for the complex64 512-point pass.)
@@ -518,16 +537,16 @@ constexpr int fast_pf_min_blocks() {
   return sizeof(T) == 4 ? (L <= 256 ? 4 : (L == 512 ? 3 : 1)) : (L <= 256 ? 5 : 2);
 }
 // FETCH = 256 (column tiles): the tile's own loads ask for 256-byte L2
-// fetches; ahead = 0: no prefetch.
+// fetches; ahead = 0: no prefetch; bulk: row prefetches as bulk copies.
 template <typename T, int L, int R0, int R1, int R2, int NT, bool IN_ROW, int FETCH = 0>
 __global__ void __launch_bounds__(NT, fast_pf_min_blocks<T, L>())
     k_fft_fast_pf(const __grid_constant__ PassGeom g, const typename Cx<T>::type* in,
                   typename Cx<T>::type* out, const __grid_constant__ PassTables<typename Cx<T>::type> tb,
-                  int64_t ahead) {
+                  int64_t ahead, int bulk) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float4* sm = reinterpret_cast<float4*>(smem_raw);
   const int64_t nt = (int64_t)blockIdx.x + ahead;
-  if (ahead > 0 && nt < g.ntiles) fast_prefetch<T, L, NT, IN_ROW>(g, in, nt);
+  if (ahead > 0 && nt < g.ntiles) fast_prefetch<T, L, NT, IN_ROW>(g, in, nt, bulk != 0);
   FastRegs<T, L, R0, R1, R2, NT> R;
   fast_load<T, L, R0, R1, R2, NT, IN_ROW, false, 0, FETCH>(g, in, blockIdx.x, sm, LD_STREAM, R);
   fast_finish<T, L, R0, R1, R2, NT, IN_ROW, LD_STREAM, ST_STREAM, false>(g, in, out, tb, blockIdx.x, sm, R,

@@ -281,6 +281,19 @@ static int prefetch_quarters(bool in_row) {
   return v[in_row ? 1 : 0];
 }
 
+// SHAFFT_SM100_BULK_PREFETCH (default 1): the row-input prefetches of
+// k_fft_fast_pf as one bulk asynchronous prefetch per row (4 KiB for the
+// complex64 512-point pass); 0: one prefetch per 128-byte line.  Measured on
+// B200 (512^3 complex64, same box, two repetitions): 2.504 / 2.507 ms per
+// step against 2.508 / 2.521 ms with the per-line prefetches.
+static int bulk_prefetch() {
+  static const int on = [] {
+    const char* e = getenv("SHAFFT_SM100_BULK_PREFETCH");
+    return (e && atoi(e) == 0) ? 0 : 1;
+  }();
+  return on;
+}
+
 // SHAFFT_SM100_COL_FETCH = 256 (default 0): the complex64 512-point passes
 // with column input load with 256-byte L2 fetches (k_fft_fast_pf<..., 256>).
 static bool col_fetch_256() {
@@ -324,11 +337,12 @@ struct FastPf {
       const int64_t resident = (int64_t)sms * fast_pf_min_blocks<T, L>();
       const int64_t ahead = q == 0 ? 0 : std::max<int64_t>(1, resident * q / 4);
       if (in_row)
-        k_fft_fast_pf<T, L, A, B, C_, NT, true><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
+        k_fft_fast_pf<T, L, A, B, C_, NT, true>
+            <<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead, bulk_prefetch());
       else if (fetch)
-        k_fft_fast_pf<T, L, A, B, C_, NT, false, 256><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
+        k_fft_fast_pf<T, L, A, B, C_, NT, false, 256><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead, 0);
       else
-        k_fft_fast_pf<T, L, A, B, C_, NT, false><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead);
+        k_fft_fast_pf<T, L, A, B, C_, NT, false><<<grid, NT, L * 128, s>>>(g, in, out, tb, ahead, 0);
       return true;
     }
     return false;

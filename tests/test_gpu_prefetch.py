@@ -4,7 +4,9 @@ against the plain kernel (SHAFFT_SM100_PREFETCH_ROW=0): the prefetch only
 warms L2, the butterflies are the same, so the outputs must be
 bit-identical.  A third run also prefetches the column-input passes
 (SHAFFT_SM100_PREFETCH_COL=4); a fourth loads the column-input passes with
-256-byte L2 fetches instead (SHAFFT_SM100_COL_FETCH=256).  The switches are
+256-byte L2 fetches instead (SHAFFT_SM100_COL_FETCH=256); a fifth issues the
+row prefetches one 128-byte line at a time instead of as one bulk
+asynchronous prefetch per row (SHAFFT_SM100_BULK_PREFETCH=0).  The switches are
 read once per process, so each setting runs in a child process.  Every result is also checked against
 the oracle (1e-6*log2(N)).  The shapes cover the transposing pair of a 3-D
 plan with few and many tiles (the prefetch target past the last tile is
@@ -58,7 +60,8 @@ t.run_all(sys.argv[2])
 def _child(tmp_path, name, **env):
     d = tmp_path / name
     d.mkdir()
-    e = {k: v for k, v in os.environ.items() if not k.startswith("SHAFFT_SM100_PREFETCH")}
+    e = {k: v for k, v in os.environ.items()
+         if not k.startswith(("SHAFFT_SM100_PREFETCH", "SHAFFT_SM100_BULK_PREFETCH", "SHAFFT_SM100_COL_FETCH"))}
     e.update(env)
     script = tmp_path / "child.py"
     script.write_text(CHILD)
@@ -72,6 +75,7 @@ def test_prefetching_pass_matches_plain_pass_bitwise(tmp_path):
     off = _child(tmp_path, "off", SHAFFT_SM100_PREFETCH_ROW="0")
     col = _child(tmp_path, "col", SHAFFT_SM100_PREFETCH_COL="4")
     fetch = _child(tmp_path, "fetch", SHAFFT_SM100_COL_FETCH="256")
+    lines = _child(tmp_path, "lines", SHAFFT_SM100_BULK_PREFETCH="0")
     for i, dims in enumerate(CASES):
         # the default prefetches every 512-point row pass, and only those
         pf_on, pf_off, pf_col = (np.load(d / f"c{i}_pf.npy") for d in (on, off, col))
@@ -89,6 +93,8 @@ def test_prefetching_pass_matches_plain_pass_bitwise(tmp_path):
             assert np.array_equal(y_col.view(np.uint32), y_off.view(np.uint32)), (dims, direction)
             y_fetch = np.load(fetch / f"c{i}_d{direction}.npy")
             assert np.array_equal(y_fetch.view(np.uint32), y_off.view(np.uint32)), (dims, direction)
+            y_lines = np.load(lines / f"c{i}_d{direction}.npy")
+            assert np.array_equal(y_lines.view(np.uint32), y_off.view(np.uint32)), (dims, direction)
             if direction == 0:
                 assert o.rel_l2(y_on, ref) <= tol, dims
             else:
