@@ -148,14 +148,14 @@ static bool tma_map_for(const PassGeom& g, const void* in, int csize, CUtensorMa
   return r == CUDA_SUCCESS;
 }
 
+// SMs of the current device (queried per call: a process may drive devices
+// of different sizes).
 static unsigned sm_count() {
-  static const unsigned n = [] {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return (unsigned)std::max(1, sms);
-  }();
-  return n;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    sms = 148;
+  return (unsigned)std::max(1, sms);
 }
 
 // Lengths with a fused two-axis plane kernel (k_fft_plane_flow).
@@ -330,11 +330,7 @@ struct FastPf {
       if (q == 0 && !fetch) return false;
       // resident CTAs on the current device: its SMs x the CTAs per SM the
       // kernel is compiled for (its 64 KiB tile fits that many)
-      int dev = 0, sms = 148;
-      if (cudaGetDevice(&dev) != cudaSuccess ||
-          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-        sms = 148;
-      const int64_t resident = (int64_t)sms * fast_pf_min_blocks<T, L>();
+      const int64_t resident = (int64_t)sm_count() * fast_pf_min_blocks<T, L>();
       const int64_t ahead = q == 0 ? 0 : std::max<int64_t>(1, resident * q / 4);
       if (in_row)
         k_fft_fast_pf<T, L, A, B, C_, NT, true>
