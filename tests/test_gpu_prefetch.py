@@ -6,9 +6,9 @@ bit-identical.  A third run also prefetches the column-input passes
 (SHAFFT_SM100_PREFETCH_COL=4); a fourth loads the column-input passes with
 256-byte L2 fetches instead (SHAFFT_SM100_COL_FETCH=256); a fifth issues the
 row prefetches one 128-byte line at a time instead of as one bulk
-asynchronous prefetch per row (SHAFFT_SM100_BULK_PREFETCH=0).  The switches are
-read once per process, so each setting runs in a child process.  Every result is also checked against
-the oracle (1e-6*log2(N)).  The shapes cover the transposing pair of a 3-D
+asynchronous prefetch per row (SHAFFT_SM100_BULK_PREFETCH=0).  The
+switches are read once per process, so each setting runs in a child
+process.  Every result is also checked against the oracle (1e-6*log2(N)).  The shapes cover the transposing pair of a 3-D
 plan with few and many tiles (the prefetch target past the last tile is
 skipped), a row pass followed by other lengths, and the four-step twiddled
 row pass of a 1-D plan."""
@@ -60,8 +60,8 @@ t.run_all(sys.argv[2])
 def _child(tmp_path, name, **env):
     d = tmp_path / name
     d.mkdir()
-    e = {k: v for k, v in os.environ.items()
-         if not k.startswith(("SHAFFT_SM100_PREFETCH", "SHAFFT_SM100_BULK_PREFETCH", "SHAFFT_SM100_COL_FETCH"))}
+    switches = ("SHAFFT_SM100_PREFETCH", "SHAFFT_SM100_BULK_PREFETCH", "SHAFFT_SM100_COL_FETCH")
+    e = {k: v for k, v in os.environ.items() if not k.startswith(switches)}
     e.update(env)
     script = tmp_path / "child.py"
     script.write_text(CHILD)
